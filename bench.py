@@ -1,0 +1,401 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 Swendsen-Wang engine; prints ONE JSON line on rank 0.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+A step is one Swendsen-Wang sweep over the whole workload.  Workloads (synthetic, seeded):
+
+  batched      512 periodic lattices, side L uniform in {64, 96, 128, 192, 256, 384, 512},
+               T uniform in [2.0, 2.6], hot start per lattice seed, one batched sweep per
+               step (the headline workload, about 40 M sites)
+  plain16384   one 16384^2 lattice at T_c, tile 16x8, lcg32 W = 16, hot start
+  plain1024    one 1024^2 lattice at T_c, tile 8x8, lcg32 W = 16, hot start
+
+`value` is spin-updates/s of the whole job with the spins resident in HBM; `e2e` is the same
+metric through the C ABI with HOST spin buffers (copies in the timed region).  The reference
+arm (--impl reference) times the reference's own CPU path (built from its sources under
+oracle/_ref) on this host's cores, on the same workload.
+
+Multi-GPU: one process per GPU (torchrun); every rank sweeps its own copy of the workload
+(weak scaling, no collective on the data path); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+T_C = 2.2691853
+MIX_SIDES = (64, 96, 128, 192, 256, 384, 512)
+MIX_COUNT = 512
+MIX_SEED = 20260
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+# ---------------------------------------------------------------------------------------------
+# workloads
+
+def mix_workload(count: int = MIX_COUNT, seed: int = MIX_SEED):
+    rng = np.random.default_rng(seed)
+    sides = rng.choice(MIX_SIDES, size=count)
+    temps = rng.uniform(2.0, 2.6, size=count).astype(np.float32)
+    seeds = rng.integers(1, 2 ** 31 - 1, size=count)
+    return [(int(L), float(T), int(s)) for L, T, s in zip(sides, temps, seeds)]
+
+
+PLAIN = {
+    "plain16384": dict(L=16384, tile=(16, 8), W=16, T=T_C),
+    "plain1024": dict(L=1024, tile=(8, 8), W=16, T=T_C),
+}
+
+
+# ---------------------------------------------------------------------------------------------
+# distributed plumbing (control plane only: barrier and max-reduce of device times)
+
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------------------------
+# clocks during the timed region
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def hbm_peak() -> tuple[float, str]:
+    try:
+        with open(MEASURED_PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ---------------------------------------------------------------------------------------------
+# algorithmic bytes (roofline numerators), per site or per tile
+
+def assign_bytes(n_sites: int, n_tiles: int, W: int) -> float:
+    """k_assign: spins read (1 B/site) + block-local labels written (4 B/site) + the tile's
+    lcg32 streams read and written (W state words + W parameter bytes + 1 counter)."""
+    return n_sites * 5 + n_tiles * 2 * (W * 5 + 4)
+
+
+def flip_bytes(n_sites: int) -> float:
+    """k_flip: labels read (4 B/site) + spins read and written (2 B/site)."""
+    return n_sites * 6
+
+
+# ---------------------------------------------------------------------------------------------
+# reference arm and CPU baseline: the reference's own CPU path in a child process
+
+def _ref_width() -> int:
+    try:
+        flags = open("/proc/cpuinfo").read()
+    except OSError:
+        flags = ""
+    return 16 if " avx512f" in flags else 8
+
+
+def ref_worker(args) -> None:
+    """Child process: times SwendsenWang_2D<LCG32, CPU>::Update of the reference."""
+    from oracle import RefHarness, have_ref
+    spec = json.loads(args.ref_spec)
+    width = _ref_width()
+    if not have_ref(width):
+        print(json.dumps({"error": f"oracle/_ref/libswref{width}.so is missing"}))
+        return
+    ref = RefHarness(width)
+    sides = spec["sides"]
+    temps = spec["temps"]
+    spins = [ref.hot_start(L, L) for L in sides]
+    threads = spec["threads"]
+    ref.cpu_sweep_many(sides, temps, spins, spec["warmup"], threads)
+    secs = ref.cpu_sweep_many(sides, temps, spins, spec["sweeps"], threads)
+    sites = sum(L * L for L in sides)
+    print(json.dumps({"seconds": secs, "site_updates": sites * spec["sweeps"], "threads": threads, "W": width}))
+
+
+def run_ref_child(sides, temps, sweeps: int, warmup: int, threads: int) -> dict:
+    spec = json.dumps({"sides": list(map(int, sides)), "temps": list(map(float, temps)), "sweeps": sweeps,
+                       "warmup": warmup, "threads": threads})
+    out = subprocess.run([sys.executable, os.path.abspath(__file__), "--_ref-worker", "--ref-spec", spec],
+                         capture_output=True, text=True, timeout=900)
+    for line in reversed(out.stdout.splitlines()):
+        if line.startswith("{"):
+            return json.loads(line)
+    return {"error": (out.stderr or out.stdout)[-300:]}
+
+
+def reference_sample(workload: str, budget_s: float = 20.0):
+    """The bounded sample of the workload the CPU runs: (sides, temps, description)."""
+    if workload == "batched":
+        mix = mix_workload()
+        sides = [L for L, _, _ in mix]
+        temps = [T for _, T, _ in mix]
+        return sides, temps, f"the full {len(mix)}-lattice mix"
+    p = PLAIN[workload]
+    return [p["L"]], [p["T"]], f"one {p['L']}^2 lattice at T={p['T']}"
+
+
+def cpu_baseline(workload: str) -> dict:
+    threads = os.cpu_count() or 1
+    sides, temps, desc = reference_sample(workload)
+    probe = run_ref_child(sides, temps, 1, 1, threads)
+    if "error" in probe:
+        return {"value": None, "unit": "spin-updates/s", "cores": threads, "kind": "reference",
+                "sample": desc, "error": probe["error"]}
+    per_sweep = max(probe["seconds"], 1e-6)
+    sweeps = max(1, min(50, int(15.0 / per_sweep)))
+    r = run_ref_child(sides, temps, sweeps, 1, threads)
+    if "error" in r:
+        return {"value": None, "unit": "spin-updates/s", "cores": threads, "kind": "reference",
+                "sample": desc, "error": r["error"]}
+    return {"value": r["site_updates"] / r["seconds"], "unit": "spin-updates/s", "cores": threads,
+            "kind": "reference",
+            "sample": f"{sweeps} sweeps of {desc} after 1 warmup sweep, reference CPU path "
+                      f"(SwendsenWang_2D<LCG32, CPU>::Update, W={r['W']}, NUM_THREADS={threads})",
+            "seconds": r["seconds"]}
+
+
+def run_reference_arm(args, dist: Dist) -> None:
+    if dist.rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    sides, temps, desc = reference_sample(args.workload)
+    probe = run_ref_child(sides, temps, 1, 1, threads)
+    metric, unit = "SW spin-updates/s", "spin-updates/s"
+    if "error" in probe:
+        print(json.dumps({"impl": "reference", "unavailable": probe["error"]}))
+        return
+    per_sweep = max(probe["seconds"], 1e-6)
+    steps = args.steps
+    while steps > 1 and per_sweep * (steps + args.warmup) > 150:
+        steps -= 1
+    r = run_ref_child(sides, temps, steps, args.warmup, threads)
+    if "error" in r:
+        print(json.dumps({"impl": "reference", "unavailable": r["error"]}))
+        return
+    value = r["site_updates"] / r["seconds"]
+    line = {
+        "impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": args.gpus,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * r["seconds"] / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic", "config": workload_config(args.workload),
+        "cpu_baseline": {"value": value, "unit": unit, "cores": threads, "kind": "reference",
+                         "sample": f"{steps} sweeps of {desc}, reference CPU path, W={r['W']}"},
+        "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def workload_config(name: str) -> dict:
+    if name == "batched":
+        mix = mix_workload()
+        return {"workload": "batched SW, 512 periodic lattices, L uniform in {64,96,128,192,256,384,512}, "
+                            "T uniform in [2.0, 2.6], hot start, one sweep of every lattice per step",
+                "lattices": len(mix), "sites": sum(L * L for L, _, _ in mix), "tile": "autotuned per L",
+                "lcg_width": 16, "l2": "inputs larger than L2"}
+    p = PLAIN[name]
+    big = p["L"] * p["L"] * 5 > 126e6
+    return {"workload": f"plain SW, one periodic {p['L']}x{p['L']} lattice, T={p['T']}, hot start",
+            "tile": list(p["tile"]), "lcg_width": p["W"], "sites": p["L"] * p["L"],
+            "l2": "inputs larger than L2" if big else "L2 flushed between timed sweeps"}
+
+
+# ---------------------------------------------------------------------------------------------
+# our arm
+
+def bench_plain(args, dist: Dist, cp) -> dict:
+    p = PLAIN[args.workload]
+    L, tile, W, T = p["L"], p["tile"], p["W"], p["T"]
+    n = L * L
+    sw = cp.SwendsenWang2D(L, L, tile, W, seed_base=1, device=dist.local_rank)
+    sw.hot_start(1)
+    sw.update(T, args.warmup)
+    sw.synchronize()
+    big = n * 5 > 126e6
+    flush = None
+    if not big:
+        flush = cp.SwendsenWang2D(4096, 4096, (16, 8), 16, device=dist.local_rank)  # 16 MB spins + 64 MB labels
+    launches0 = cp.kernel_launches()
+    dist.barrier()
+    with ClockSampler(dist.local_rank) as clocks:
+        if big:
+            ms = float(sw.sweep_timed(T, args.steps)[0])
+        else:
+            ms = 0.0
+            for _ in range(args.steps):
+                flush.cold_start(0)
+                flush.cold_start(1)
+                flush.synchronize()
+                ms += float(sw.sweep_timed(T, 1)[0])
+    launches = cp.kernel_launches() - launches0 - (0 if big else 2 * args.steps)
+    dist.barrier()
+    ms_max = dist.max(ms)
+    value = dist.world * n * args.steps / (ms_max / 1e3)
+    # per-kernel times for the roofline (separate instrumented pass)
+    k = sw.sweep_timed(T, max(3, min(args.steps, 20)), per_kernel=True)
+    nk = max(3, min(args.steps, 20))
+    n_tiles, _ = sw.rng_shape()
+    peak, peak_kind = hbm_peak()
+    a_ms = float(k[1]) / nk
+    ab = assign_bytes(n, n_tiles, W)
+    fb = flip_bytes(n)
+    # e2e through host buffers
+    spins_in = cp.lattice.pinned_empty((L, L), np.uint8)
+    spins_out = cp.lattice.pinned_empty((L, L), np.uint8)
+    spins_in[:] = sw.get_spins()
+    em = np.zeros(2)
+    import time as _t
+    sw.update_host(T, spins_in, spins_out, em)
+    e2e_steps = max(3, min(args.steps, 10))
+    dist.barrier()
+    t0 = _t.perf_counter()
+    for _ in range(e2e_steps):
+        sw.update_host(T, spins_in, spins_out, em)
+        spins_in, spins_out = spins_out, spins_in
+    e2e_s = dist.max(_t.perf_counter() - t0)
+    e2e = dist.world * n * e2e_steps / e2e_s
+    sw.close()
+    return {
+        "value": value, "ms_per_step": ms_max / args.steps, "launches": launches, "clocks": clocks.summary(),
+        "roofline": {"bound": "hbm", "kernel": "k_assign", "achieved": ab / (a_ms / 1e3) / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": ab / (a_ms / 1e3) / 1e9 / peak, "traffic": None,
+                     "peak_kind": peak_kind, "bytes_per_launch": ab, "ms_per_launch": a_ms},
+        "kernels_ms_per_sweep": {"assign": a_ms, "merge": float(k[2]) / nk, "flip": float(k[3]) / nk},
+        "flip_GBs": fb / (float(k[3]) / nk / 1e3) / 1e9,
+        "e2e": {"value": e2e, "unit": "spin-updates/s", "h2d_bytes_per_step": n, "d2h_bytes_per_step": n + 16},
+    }
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="plain16384", choices=["batched", *PLAIN])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--_ref-worker", dest="ref_worker_mode", action="store_true")
+    ap.add_argument("--ref-spec", default="")
+    args = ap.parse_args()
+    if args.ref_worker_mode:
+        ref_worker(args)
+        return
+    args.warmup = max(args.warmup, 3)
+    dist = Dist()
+    try:
+        if args.impl == "reference":
+            run_reference_arm(args, dist)
+            return
+        import computational_physics_b200 as cp
+        if cp.device_count() < 1:
+            raise RuntimeError("no CUDA device")
+        r = bench_plain(args, dist, cp)
+        if dist.rank != 0:
+            return
+        line = {
+            "metric": "SW spin-updates/s", "value": r["value"], "unit": "spin-updates/s", "n_gpus": dist.world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {**workload_config(args.workload), "parallelism": f"replicas x{dist.world}"},
+            "roofline": r["roofline"], "e2e": r["e2e"], "gpu_launches": r["launches"], "clocks": r["clocks"],
+            "kernels_ms_per_sweep": r["kernels_ms_per_sweep"],
+        }
+        if dist.world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(args.workload)
+        print(json.dumps(line))
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,167 @@
+"""Many lattices on one GPU: the batched Swendsen-Wang engine (persistent kernels over a
+device work queue, one CUDA graph per round) behind the swb_batch_* C ABI."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from ._native import I32, P, U32, U64, F32, check, extra_signatures, lib
+
+extra_signatures({
+    "swb_batch_create": ([P, U32, U64, U32, I32], I32),
+    "swb_batch_destroy": ([P], I32),
+    "swb_batch_lattice_bytes": ([U32, U32, U32, U32, U32, P], I32),
+    "swb_batch_add": ([P, U32, U32, U32, U32, U32, U32, F32, U32, P], I32),
+    "swb_batch_remove": ([P, U32], I32),
+    "swb_batch_hot_start": ([P, U32, U32], I32),
+    "swb_batch_set_spins": ([P, U32, P], I32),
+    "swb_batch_get_spins": ([P, U32, P], I32),
+    "swb_batch_set_temperature": ([P, U32, F32], I32),
+    "swb_batch_set_schedule": ([P, U32, U32, U32], I32),
+    "swb_batch_status": ([P, U32, P, P], I32),
+    "swb_batch_sweep": ([P, U32, I32], I32),
+    "swb_batch_synchronize": ([P], I32),
+    "swb_batch_sweep_timed": ([P, U32, I32, P], I32),
+    "swb_batch_accumulators": ([P, U32, P], I32),
+    "swb_batch_samples": ([P, U32, P, U64, P], I32),
+    "swb_batch_get_rng": ([P, U32, P, P, P, P], I32),
+    "swb_batch_info": ([P, U32, P], I32),
+    "swb_batch_memory": ([P, P, P], I32),
+    "swb_batch_update_host": ([P, U32, P, P, P], I32),
+})
+
+UNLIMITED = 0xFFFFFFFF
+
+__all__ = ["BatchedSW", "lattice_bytes", "UNLIMITED"]
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+def lattice_bytes(L0: int, L1: int, tile=(16, 8), lcg_width: int = 16) -> int:
+    v = ctypes.c_uint64()
+    check(lib().swb_batch_lattice_bytes(L0, L1, tile[0], tile[1], lcg_width, ctypes.byref(v)))
+    return v.value
+
+
+class BatchedSW:
+    """Independent periodic lattices of different sizes, tiles and temperatures, swept
+    together.  Each lattice is bit-identical to a :class:`SwendsenWang2D` with the same
+    extent, tile, lcg width and seed base."""
+
+    def __init__(self, capacity: int = 1024, hbm_budget_bytes: int = 0, lcg_width: int = 16, device: int = 0):
+        self._lib = lib()
+        h = ctypes.c_void_p()
+        check(self._lib.swb_batch_create(ctypes.byref(h), capacity, hbm_budget_bytes, lcg_width, device))
+        self._h = h
+        self.lcg_width = lcg_width
+        self.shapes: dict[int, tuple[int, int]] = {}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.swb_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def add(self, L0: int, L1: int | None = None, temperature: float = 2.2691853, seed_base: int = 1,
+            tile=(16, 8), block=(0, 0)) -> int:
+        L1 = L0 if L1 is None else L1
+        i = ctypes.c_uint32()
+        check(self._lib.swb_batch_add(self._h, L0, L1, tile[0], tile[1], block[0], block[1], temperature,
+                                      seed_base, ctypes.byref(i)))
+        self.shapes[i.value] = (L1, L0)
+        return i.value
+
+    def remove(self, lid: int) -> None:
+        check(self._lib.swb_batch_remove(self._h, lid))
+        self.shapes.pop(lid, None)
+
+    def hot_start(self, lid: int, seed: int = 1) -> None:
+        check(self._lib.swb_batch_hot_start(self._h, lid, seed))
+
+    def set_spins(self, lid: int, spins: np.ndarray) -> None:
+        s = np.ascontiguousarray(spins, np.uint8)
+        if s.size != int(np.prod(self.shapes[lid])):
+            raise ValueError("wrong number of spins")
+        check(self._lib.swb_batch_set_spins(self._h, lid, _ptr(s)))
+
+    def get_spins(self, lid: int) -> np.ndarray:
+        out = np.empty(self.shapes[lid], np.uint8)
+        check(self._lib.swb_batch_get_spins(self._h, lid, _ptr(out)))
+        return out
+
+    def set_temperature(self, lid: int, temperature: float) -> None:
+        check(self._lib.swb_batch_set_temperature(self._h, lid, temperature))
+
+    def set_schedule(self, lid: int, sweeps: int = UNLIMITED, measure_every: int = 0) -> None:
+        check(self._lib.swb_batch_set_schedule(self._h, lid, sweeps, measure_every))
+
+    def status(self, lid: int) -> tuple[int, int]:
+        left = ctypes.c_uint32()
+        done = ctypes.c_uint32()
+        check(self._lib.swb_batch_status(self._h, lid, ctypes.byref(left), ctypes.byref(done)))
+        return left.value, done.value
+
+    def sweep(self, rounds: int = 1, measure: bool = False) -> None:
+        check(self._lib.swb_batch_sweep(self._h, rounds, int(measure)))
+
+    def synchronize(self) -> None:
+        check(self._lib.swb_batch_synchronize(self._h))
+
+    def sweep_timed(self, rounds: int, per_kernel: bool = False) -> np.ndarray:
+        ms = np.zeros(4, np.float32)
+        check(self._lib.swb_batch_sweep_timed(self._h, rounds, int(per_kernel), _ptr(ms)))
+        return ms
+
+    def accumulators(self, lid: int) -> np.ndarray:
+        out = np.zeros(4, np.float64)
+        check(self._lib.swb_batch_accumulators(self._h, lid, _ptr(out)))
+        return out
+
+    def samples(self, lid: int) -> np.ndarray:
+        n = ctypes.c_uint64()
+        check(self._lib.swb_batch_samples(self._h, lid, None, 0, ctypes.byref(n)))
+        out = np.empty((n.value, 2), np.int64)
+        check(self._lib.swb_batch_samples(self._h, lid, _ptr(out), n.value, ctypes.byref(n)))
+        return out
+
+    def get_rng(self, lid: int):
+        g = self.info(lid)
+        nt, w = g["tiles"], self.lcg_width
+        st = np.empty((nt, w), np.uint32); a = np.empty((nt, w), np.uint32); c = np.empty((nt, w), np.uint32)
+        it = np.empty(nt, np.uint32)
+        check(self._lib.swb_batch_get_rng(self._h, lid, _ptr(st), _ptr(a), _ptr(c), _ptr(it)))
+        return st, a, c, it
+
+    def info(self, lid: int) -> dict:
+        v = np.zeros(8, np.uint32)
+        check(self._lib.swb_batch_info(self._h, lid, _ptr(v)))
+        keys = ("L0", "L1", "tile_x", "tile_y", "block_x", "block_y", "tiles", "blocks")
+        return {k: int(x) for k, x in zip(keys, v)}
+
+    def memory(self) -> tuple[int, int]:
+        used = ctypes.c_uint64()
+        budget = ctypes.c_uint64()
+        check(self._lib.swb_batch_memory(self._h, ctypes.byref(used), ctypes.byref(budget)))
+        return used.value, budget.value
+
+    def update_host(self, ids, spins_in, spins_out) -> None:
+        k = len(ids)
+        idarr = np.asarray(ids, np.uint32)
+        pin = (ctypes.c_void_p * k)(*[s.ctypes.data for s in spins_in])
+        pout = (ctypes.c_void_p * k)(*[s.ctypes.data for s in spins_out])
+        check(self._lib.swb_batch_update_host(self._h, k, _ptr(idarr), ctypes.cast(pin, ctypes.c_void_p),
+                                              ctypes.cast(pout, ctypes.c_void_p)))

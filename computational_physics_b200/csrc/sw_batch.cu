@@ -1,0 +1,912 @@
+// Batched Swendsen-Wang: hundreds of independent periodic lattices of different sizes,
+// tiles and temperatures advance together, one persistent kernel per sweep phase.
+//
+// Work queue.  Every active lattice contributes its blocks (TBX x TBY tiles) to one flat list
+// of work items; a lattice's items follow the exclusive prefix sum blk_prefix.  The persistent
+// CTAs of kb_assign / kb_merge pull items from a device counter (atomicAdd) until the list is
+// exhausted; kb_flip and kb_measure do the same over chunks of 4096 sites.  Each phase resets
+// the counter of the phase that ran before it, so a sweep needs no host work and the whole
+// sweep is one CUDA graph, captured once per handle and replayed: the graph reads the item
+// totals from device memory, so adding or removing lattices does not invalidate it.
+//
+// Per lattice the device keeps spins, labels, lcg32 streams (one per tile, seeded
+// seed_base + tile id as the reference's CPU path with one stream per tile), a sweep budget
+// (sweeps_left, decremented on the device; lattices at 0 are skipped) and FP64 observable
+// accumulators, so jobs with different sweep counts share the same graph replays.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <vector>
+
+#include "sw_core.cuh"
+
+namespace swb {
+
+constexpr uint32_t kBatchThreads = 512;        // CTA size of the persistent kernels
+constexpr uint32_t kChunkSites = 4096;         // flip / measure work item
+constexpr uint32_t kUnlimited = 0xFFFFFFFFu;   // sweeps_left value that never runs out
+
+struct BatchLat {
+    Geo g;
+    uint8_t *spins;
+    uint32_t *labels;
+    uint32_t *rng_state;
+    uint8_t *rng_sel;
+    uint32_t *rng_iter;
+    uint32_t *edge;
+    Obs *obs;
+    long long *series;
+    unsigned long long series_cap;
+    float p_add;
+    uint32_t sweeps_left;     // sweeps still to run (kUnlimited: no limit)
+    uint32_t swept;           // 1 if this lattice was swept in the current round
+    uint32_t measure_every;   // measure after every measure_every-th sweep (0: never)
+    uint32_t sweeps_done;     // sweeps completed
+    uint32_t chunks_left;     // flip chunks not yet done in this round
+};
+
+struct BatchCounters {
+    unsigned int queue[4];    // assign, merge, flip, measure
+    unsigned int n_active;    // lattices in the work lists
+    unsigned int total_blocks;
+    unsigned int total_chunks;
+    unsigned int pad;
+};
+
+// Lattice of work item `item`: largest k with prefix[k] <= item.
+__device__ __forceinline__ uint32_t find_lattice(const uint32_t *prefix, uint32_t n, uint32_t item)
+{
+    uint32_t lo = 0, hi = n;  // prefix[lo] <= item < prefix[hi]
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (prefix[mid] <= item)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ uint32_t next_item(unsigned int *queue, uint32_t *slot)
+{
+    if (threadIdx.x == 0)
+        *slot = atomicAdd(queue, 1u);
+    __syncthreads();
+    const uint32_t item = *slot;
+    __syncthreads();
+    return item;
+}
+
+template <int W>
+__global__ void __launch_bounds__(kBatchThreads) kb_assign(BatchLat *lats, const uint32_t *active, const uint32_t *blk_prefix,
+                                                           BatchCounters *ctr)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ uint32_t slot;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctr->queue[2] = 0;  // flip and measure of the previous round are finished
+        ctr->queue[3] = 0;
+    }
+    const uint32_t n = ctr->n_active, total = ctr->total_blocks;
+    while (true) {
+        const uint32_t item = next_item(&ctr->queue[0], &slot);
+        if (item >= total)
+            break;
+        const uint32_t k = find_lattice(blk_prefix, n, item);
+        BatchLat *L = lats + active[k];
+        if (L->sweeps_left == 0)
+            continue;
+        const Geo g = L->g;
+        const uint32_t blk = item - blk_prefix[k];
+        assign_block<W>(g, blk % g.nbx, blk / g.nbx, L->spins, L->labels, L->rng_state, L->rng_sel, L->rng_iter,
+                        L->p_add, L->edge, nullptr, nullptr, smem);
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kBatchThreads) kb_merge(BatchLat *lats, const uint32_t *active, const uint32_t *blk_prefix,
+                                                          BatchCounters *ctr)
+{
+    __shared__ uint32_t slot;
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        ctr->queue[0] = 0;
+    const uint32_t n = ctr->n_active, total = ctr->total_blocks;
+    while (true) {
+        const uint32_t item = next_item(&ctr->queue[1], &slot);
+        if (item >= total)
+            break;
+        const uint32_t k = find_lattice(blk_prefix, n, item);
+        BatchLat *L = lats + active[k];
+        if (L->sweeps_left == 0)
+            continue;
+        const Geo g = L->g;
+        if (threadIdx.x < g.BX + g.BY)
+            merge_block(g, item - blk_prefix[k], threadIdx.x, L->edge, L->labels);
+    }
+}
+
+// Resolve + flip of one chunk; the last chunk of a lattice closes its round (sweep budget).
+__global__ void __launch_bounds__(kBatchThreads) kb_flip(BatchLat *lats, const uint32_t *active, const uint32_t *chunk_prefix,
+                                                         BatchCounters *ctr)
+{
+    __shared__ uint32_t slot;
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        ctr->queue[1] = 0;
+    const uint32_t n = ctr->n_active, total = ctr->total_chunks;
+    while (true) {
+        const uint32_t item = next_item(&ctr->queue[2], &slot);
+        if (item >= total)
+            break;
+        const uint32_t k = find_lattice(chunk_prefix, n, item);
+        BatchLat *L = lats + active[k];
+        if (L->sweeps_left == 0)
+            continue;
+        const size_t nsites = (size_t)L->g.L0 * L->g.L1;
+        const size_t q0 = (size_t)(item - chunk_prefix[k]) * (kChunkSites / 4);
+        const size_t q1 = min(q0 + kChunkSites / 4, nsites / 4);
+        const uint32_t *labels = L->labels;
+        for (size_t q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
+            const uint4 lab = reinterpret_cast<const uint4 *>(labels)[q];
+            const uint32_t r[4] = {lab.x, lab.y, lab.z, lab.w};
+            uint32_t flip = 0;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                uint32_t c = r[j], d;
+                while ((d = labels[c]) != c)
+                    c = d;
+                flip |= (c & 1u) << (8 * j);
+            }
+            reinterpret_cast<uint32_t *>(L->spins)[q] ^= flip;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            if (atomicSub(&L->chunks_left, 1u) == 1u) {
+                // last chunk of this lattice in this round
+                const uint32_t nchunks = chunk_prefix[k + 1] - chunk_prefix[k];
+                L->chunks_left = nchunks;
+                L->swept = 1;
+                L->sweeps_done += 1;
+                if (L->sweeps_left != kUnlimited)
+                    L->sweeps_left -= 1;
+            }
+        }
+    }
+}
+
+// Energy / magnetisation of lattices that completed a multiple of measure_every sweeps in
+// this round; per-lattice int64 sums, the last chunk turns them into FP64 accumulators.
+__global__ void __launch_bounds__(kBatchThreads) kb_measure(BatchLat *lats, const uint32_t *active,
+                                                            const uint32_t *chunk_prefix, BatchCounters *ctr)
+{
+    __shared__ uint32_t slot;
+    __shared__ long long se[kBatchThreads / 32], sm[kBatchThreads / 32];
+    const uint32_t n = ctr->n_active, total = ctr->total_chunks;
+    while (true) {
+        const uint32_t item = next_item(&ctr->queue[3], &slot);
+        if (item >= total)
+            break;
+        const uint32_t k = find_lattice(chunk_prefix, n, item);
+        BatchLat *L = lats + active[k];
+        if (!L->swept || L->measure_every == 0 || (L->sweeps_done % L->measure_every) != 0)
+            continue;
+        const uint32_t L0 = L->g.L0, L1 = L->g.L1;
+        const size_t nsites = (size_t)L0 * L1;
+        const size_t i0 = (size_t)(item - chunk_prefix[k]) * kChunkSites;
+        const size_t i1 = min(i0 + kChunkSites, nsites);
+        const uint8_t *s = L->spins;
+        long long e = 0, m = 0;
+        for (size_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+            const uint32_t y = (uint32_t)(i / L0), x = (uint32_t)(i - (size_t)y * L0);
+            const int v = 2 * s[i] - 1;
+            const int r = 2 * s[(size_t)y * L0 + (x + 1 == L0 ? 0 : x + 1)] - 1;
+            const int d = 2 * s[(size_t)(y + 1 == L1 ? 0 : y + 1) * L0 + x] - 1;
+            e += v * (r + d);
+            m += v;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            e += __shfl_xor_sync(0xffffffffu, e, o);
+            m += __shfl_xor_sync(0xffffffffu, m, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            se[threadIdx.x >> 5] = e;
+            sm[threadIdx.x >> 5] = m;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            long long be = 0, bm = 0;
+            for (uint32_t w = 0; w < blockDim.x / 32; ++w) {
+                be += se[w];
+                bm += sm[w];
+            }
+            Obs *o = L->obs;
+            atomicAdd(&o->e, (unsigned long long)be);
+            atomicAdd(&o->m, (unsigned long long)bm);
+            __threadfence();
+            const uint32_t nchunks = chunk_prefix[k + 1] - chunk_prefix[k];
+            if (atomicAdd(&o->done, 1u) == nchunks - 1) {
+                __threadfence();
+                const long long te = (long long)atomicAdd(&o->e, 0ull);
+                const long long tm = (long long)atomicAdd(&o->m, 0ull);
+                o->last_e = te;
+                o->last_m = tm;
+                const double E = -(double)te / (double)nsites, M = (double)tm / (double)nsites;
+                o->acc[0] += E;
+                o->acc[1] += E * E;
+                o->acc[2] += fabs(M);
+                o->acc[3] += 1.0;
+                const unsigned long long j = o->n_samples;
+                if (j < L->series_cap) {
+                    L->series[2 * j] = te;
+                    L->series[2 * j + 1] = tm;
+                }
+                o->n_samples = j + 1;
+                o->e = 0;
+                o->m = 0;
+                o->done = 0;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Clears the per-round "swept" flags (first node of a round).
+__global__ void kb_begin_round(BatchLat *lats, const uint32_t *active, BatchCounters *ctr)
+{
+    const uint32_t n = ctr->n_active;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        lats[active[k]].swept = 0;
+}
+
+template <int W>
+__global__ void kb_rng_init(const uint32_t n_tiles, const uint32_t seed_base, uint32_t *state, uint8_t *sel,
+                            uint32_t *iter)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_tiles)
+        return;
+    uint64_t x = drand48_seed(seed_base + t);
+    uint32_t s[W];
+#pragma unroll
+    for (int i = 0; i < W; ++i) {
+        x = drand48_step(x);
+        s[i] = ((uint32_t)__dmul_rn(1000.0, drand48_value(x))) % 5u;
+        sel[(size_t)t * W + i] = (uint8_t)s[i];
+    }
+    x = drand48_step(x);
+    uint32_t v = lcg_param_a(s[0]) * ((uint32_t)__dmul_rn(4026531839.0, drand48_value(x)) + 1u) + lcg_param_c(s[0]);
+    state[(size_t)t * W] = v;
+#pragma unroll
+    for (int i = 1; i < W; ++i) {
+        v = lcg_param_a(s[i]) * v + lcg_param_c(s[i]);
+        state[(size_t)t * W + i] = v;
+    }
+    iter[t] = 0;
+}
+
+__global__ void kb_hot_start(const size_t n, const uint32_t seed, uint8_t *spins)
+{
+    constexpr uint32_t kChunk = 64;
+    const size_t first = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) * kChunk;
+    if (first >= n)
+        return;
+    uint64_t A, C;
+    drand48_jump(first, A, C);
+    uint64_t x = (A * drand48_seed(seed) + C) & kDrandMask;
+    const size_t last = first + kChunk < n ? first + kChunk : n;
+    for (size_t i = first; i < last; ++i) {
+        x = drand48_step(x);
+        spins[i] = (uint8_t)(x >> 47);
+    }
+}
+
+}  // namespace swb
+
+using namespace swb;
+
+namespace {
+
+struct HostLat {
+    bool used = false;
+    BatchLat d{};             // host copy of the descriptor
+    uint64_t bytes = 0;       // device bytes held
+    void *mem = nullptr;      // one allocation for all buffers of the lattice
+};
+
+}  // namespace
+
+struct swb_batch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint32_t W = 16, capacity = 0;
+    uint64_t budget = 0, used = 0;
+    std::vector<HostLat> lats;
+    BatchLat *d_lats = nullptr;
+    uint32_t *d_active = nullptr, *d_blk_prefix = nullptr, *d_chunk_prefix = nullptr;
+    BatchCounters *d_ctr = nullptr;
+    std::vector<uint32_t> active;   // ids in the work lists
+    bool lists_dirty = true;
+    int grid_assign = 0, grid_other = 0;
+    uint32_t smem_assign = 0;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};   // [measure?]
+    uint64_t series_cap = 1u << 16;
+};
+
+namespace {
+
+int bset_device(const swb_batch *b)
+{
+    SWB_CUDA(cudaSetDevice(b->device));
+    return SWB_OK;
+}
+
+uint32_t lattice_chunks(const Geo &g) { return (uint32_t)(((size_t)g.L0 * g.L1 + kChunkSites - 1) / kChunkSites); }
+
+// Device bytes one lattice needs (the admission estimate).
+uint64_t lattice_bytes(const Geo &g, uint32_t W, uint64_t series_cap)
+{
+    const uint64_t n = (uint64_t)g.L0 * g.L1, tiles = (uint64_t)g.n0 * g.n1, blocks = (uint64_t)g.nbx * g.nby;
+    auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
+    return al(n) + al(4 * n) + al(4 * tiles * W) + al(tiles * W) + al(4 * tiles) + al(4 * kEdgeWords * blocks) +
+           al(sizeof(Obs)) + al(16 * series_cap);
+}
+
+int upload_descriptor(swb_batch *b, uint32_t id)
+{
+    SWB_CUDA(cudaMemcpyAsync(b->d_lats + id, &b->lats[id].d, sizeof(BatchLat), cudaMemcpyHostToDevice, b->stream));
+    return SWB_OK;
+}
+
+// Rebuilds the active list and prefix sums (host) and uploads them with the totals.
+int rebuild_lists(swb_batch *b)
+{
+    if (!b->lists_dirty)
+        return SWB_OK;
+    b->active.clear();
+    for (uint32_t i = 0; i < b->capacity; ++i)
+        if (b->lats[i].used)
+            b->active.push_back(i);
+    // big lattices first: their many items start early and balance the tail
+    std::stable_sort(b->active.begin(), b->active.end(), [&](uint32_t x, uint32_t y) {
+        const Geo &gx = b->lats[x].d.g, &gy = b->lats[y].d.g;
+        return (uint64_t)gx.L0 * gx.L1 > (uint64_t)gy.L0 * gy.L1;
+    });
+    const uint32_t n = (uint32_t)b->active.size();
+    std::vector<uint32_t> bp(n + 1, 0), cp(n + 1, 0);
+    for (uint32_t k = 0; k < n; ++k) {
+        const Geo &g = b->lats[b->active[k]].d.g;
+        bp[k + 1] = bp[k] + g.nbx * g.nby;
+        cp[k + 1] = cp[k] + lattice_chunks(g);
+    }
+    BatchCounters c{};
+    c.n_active = n;
+    c.total_blocks = bp[n];
+    c.total_chunks = cp[n];
+    if (n) {
+        SWB_CUDA(cudaMemcpyAsync(b->d_active, b->active.data(), n * 4, cudaMemcpyHostToDevice, b->stream));
+        SWB_CUDA(cudaMemcpyAsync(b->d_blk_prefix, bp.data(), (n + 1) * 4, cudaMemcpyHostToDevice, b->stream));
+        SWB_CUDA(cudaMemcpyAsync(b->d_chunk_prefix, cp.data(), (n + 1) * 4, cudaMemcpyHostToDevice, b->stream));
+    }
+    SWB_CUDA(cudaMemcpyAsync(b->d_ctr, &c, sizeof(c), cudaMemcpyHostToDevice, b->stream));
+    b->lists_dirty = false;
+    return SWB_OK;
+}
+
+template <int W>
+int launch_round_w(swb_batch *b, bool measure)
+{
+    kb_begin_round<<<4, 128, 0, b->stream>>>(b->d_lats, b->d_active, b->d_ctr);
+    SWB_LAUNCHED();
+    kb_assign<W><<<b->grid_assign, kBatchThreads, b->smem_assign, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix,
+                                                                              b->d_ctr);
+    SWB_LAUNCHED();
+    kb_merge<<<b->grid_other, kBatchThreads, 0, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix, b->d_ctr);
+    SWB_LAUNCHED();
+    kb_flip<<<b->grid_other, kBatchThreads, 0, b->stream>>>(b->d_lats, b->d_active, b->d_chunk_prefix, b->d_ctr);
+    SWB_LAUNCHED();
+    if (measure) {
+        kb_measure<<<b->grid_other, kBatchThreads, 0, b->stream>>>(b->d_lats, b->d_active, b->d_chunk_prefix,
+                                                                   b->d_ctr);
+        SWB_LAUNCHED();
+    }
+    return SWB_OK;
+}
+
+int launch_round(swb_batch *b, bool measure)
+{
+    switch (b->W) {
+    case 8: return launch_round_w<8>(b, measure);
+    case 16: return launch_round_w<16>(b, measure);
+    case 32: return launch_round_w<32>(b, measure);
+    }
+    return fail(SWB_ERR_ARGUMENT, "unsupported lcg width %u", b->W);
+}
+
+// One round captured once per handle; it stays valid because every kernel reads the
+// lattice set from device memory.
+int round_graph(swb_batch *b, bool measure, cudaGraphExec_t *out)
+{
+    cudaGraphExec_t &ge = b->graph[measure ? 1 : 0];
+    if (!ge) {
+        cudaGraph_t g = nullptr;
+        SWB_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = launch_round(b, measure);
+        const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+        if (rc)
+            return rc;
+        if (e != cudaSuccess)
+            return fail(SWB_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+        const cudaError_t e2 = cudaGraphInstantiate(&ge, g, 0);
+        cudaGraphDestroy(g);
+        if (e2 != cudaSuccess)
+            return fail(SWB_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e2));
+    }
+    *out = ge;
+    return SWB_OK;
+}
+
+HostLat *get_lat(swb_batch *b, uint32_t id)
+{
+    if (!b || id >= b->capacity || !b->lats[id].used)
+        return nullptr;
+    return &b->lats[id];
+}
+
+int rounds(swb_batch *b, uint32_t n_rounds, bool any_measure)
+{
+    if (int rc = rebuild_lists(b))
+        return rc;
+    cudaGraphExec_t ge;
+    if (int rc = round_graph(b, any_measure, &ge))
+        return rc;
+    for (uint32_t r = 0; r < n_rounds; ++r) {
+        SWB_CUDA(cudaGraphLaunch(ge, b->stream));
+        g_launches.fetch_add(any_measure ? 5 : 4, std::memory_order_relaxed);
+    }
+    return SWB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int swb_batch_lattice_bytes(uint32_t L0, uint32_t L1, uint32_t tile_x, uint32_t tile_y, uint32_t lcg_width,
+                            uint64_t *bytes)
+{
+    if (!bytes)
+        return fail(SWB_ERR_ARGUMENT, "bytes is NULL");
+    const Geo g = make_geo(L0, L1, tile_x, tile_y, lcg_width, kBatchThreads);
+    *bytes = lattice_bytes(g, lcg_width, 1u << 16);
+    return SWB_OK;
+}
+
+int swb_batch_create(swb_batch **out, uint32_t capacity, uint64_t hbm_budget_bytes, uint32_t lcg_width, int device)
+{
+    if (!out)
+        return fail(SWB_ERR_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    if (capacity == 0 || capacity > (1u << 20))
+        return fail(SWB_ERR_ARGUMENT, "capacity must be in [1, 2^20]");
+    if (!(lcg_width == 8 || lcg_width == 16 || lcg_width == 32))
+        return fail(SWB_ERR_ARGUMENT, "unsupported lcg32 width %u", lcg_width);
+    swb_batch *b = new swb_batch();
+    b->device = device;
+    b->W = lcg_width;
+    b->capacity = capacity;
+    b->budget = hbm_budget_bytes;
+    b->lats.resize(capacity);
+    auto cleanup = [&](int rc) {
+        swb_batch_destroy(b);
+        return rc;
+    };
+#define SWB_TRY(call)                                                                              \
+    do {                                                                                           \
+        cudaError_t err__ = (call);                                                                \
+        if (err__ != cudaSuccess)                                                                  \
+            return cleanup(fail(SWB_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(err__))); \
+    } while (0)
+    SWB_TRY(cudaSetDevice(device));
+    SWB_TRY(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    SWB_TRY(cudaMalloc(&b->d_lats, sizeof(BatchLat) * capacity));
+    SWB_TRY(cudaMalloc(&b->d_active, 4 * capacity));
+    SWB_TRY(cudaMalloc(&b->d_blk_prefix, 4 * (capacity + 1)));
+    SWB_TRY(cudaMalloc(&b->d_chunk_prefix, 4 * (capacity + 1)));
+    SWB_TRY(cudaMalloc(&b->d_ctr, sizeof(BatchCounters)));
+    SWB_TRY(cudaMemsetAsync(b->d_ctr, 0, sizeof(BatchCounters), b->stream));
+    SWB_TRY(cudaMemsetAsync(b->d_blk_prefix, 0, 4 * (capacity + 1), b->stream));
+    SWB_TRY(cudaMemsetAsync(b->d_chunk_prefix, 0, 4 * (capacity + 1), b->stream));
+    // The assign phase may hold any block up to 128 x 32 sites: size shared memory for it.
+    Geo gmax{};
+    gmax.BX = 128; gmax.BY = 32; gmax.TBX = 32; gmax.TBY = 1; gmax.TY = 32;
+    b->smem_assign = assign_smem(gmax).total;
+    int sms = 148, per_sm = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    switch (lcg_width) {
+    case 8: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kb_assign<8>, kBatchThreads, b->smem_assign); break;
+    case 16: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kb_assign<16>, kBatchThreads, b->smem_assign); break;
+    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kb_assign<32>, kBatchThreads, b->smem_assign); break;
+    }
+    b->grid_assign = sms * std::max(per_sm, 1);
+    int per_sm2 = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, kb_flip, kBatchThreads, 0);
+    b->grid_other = sms * std::max(per_sm2, 1);
+    SWB_TRY(cudaStreamSynchronize(b->stream));
+#undef SWB_TRY
+    *out = b;
+    return SWB_OK;
+}
+
+int swb_batch_destroy(swb_batch *b)
+{
+    if (!b)
+        return SWB_OK;
+    cudaSetDevice(b->device);
+    if (b->stream)
+        cudaStreamSynchronize(b->stream);
+    for (auto &ge : b->graph)
+        if (ge)
+            cudaGraphExecDestroy(ge);
+    for (auto &l : b->lats)
+        if (l.mem)
+            cudaFree(l.mem);
+    cudaFree(b->d_lats);
+    cudaFree(b->d_active);
+    cudaFree(b->d_blk_prefix);
+    cudaFree(b->d_chunk_prefix);
+    cudaFree(b->d_ctr);
+    if (b->stream)
+        cudaStreamDestroy(b->stream);
+    delete b;
+    return SWB_OK;
+}
+
+int swb_batch_add(swb_batch *b, uint32_t L0, uint32_t L1, uint32_t tile_x, uint32_t tile_y, uint32_t block_x,
+                  uint32_t block_y, float temperature, uint32_t seed_base, uint32_t *id)
+{
+    if (!b || !id)
+        return fail(SWB_ERR_ARGUMENT, "NULL argument");
+    if (L0 == 0 || L1 == 0 || (L0 % 2) || (L1 % 2))
+        return fail(SWB_ERR_ARGUMENT, "SwendsenWang_2D implementation requires evenly sized lattice (%u x %u)", L0, L1);
+    if ((uint64_t)L0 * L1 > 0xFFFFFFFFull)
+        return fail(SWB_ERR_ARGUMENT, "lattice of %u x %u sites exceeds 32-bit labels", L0, L1);
+    if (!(tile_x == 8 || tile_x == 16 || tile_x == 32) || tile_y < 2 || tile_y > 32)
+        return fail(SWB_ERR_ARGUMENT, "unsupported tile %u x %u", tile_x, tile_y);
+    if (!(temperature > 0.0f) || !std::isfinite(temperature))
+        return fail(SWB_ERR_ARGUMENT, "temperature must be positive and finite");
+    if (int rc = bset_device(b))
+        return rc;
+    uint32_t slot = b->capacity;
+    for (uint32_t i = 0; i < b->capacity; ++i)
+        if (!b->lats[i].used) {
+            slot = i;
+            break;
+        }
+    if (slot == b->capacity)
+        return fail(SWB_ERR_CAPACITY, "all %u lattice slots are in use", b->capacity);
+    const Geo g = make_geo(L0, L1, tile_x, tile_y, b->W, kBatchThreads, block_x, block_y);
+    if (assign_smem(g).total > b->smem_assign)
+        return fail(SWB_ERR_ARGUMENT, "block of %u x %u sites needs more shared memory than reserved", g.BX, g.BY);
+    const uint64_t bytes = lattice_bytes(g, b->W, b->series_cap);
+    if (b->budget && b->used + bytes > b->budget)
+        return fail(SWB_ERR_CAPACITY, "lattice needs %llu bytes, %llu of %llu in use", (unsigned long long)bytes,
+                    (unsigned long long)b->used, (unsigned long long)b->budget);
+    HostLat &h = b->lats[slot];
+    void *mem = nullptr;
+    SWB_CUDA(cudaMalloc(&mem, bytes));
+    const uint64_t n = (uint64_t)L0 * L1, tiles = (uint64_t)g.n0 * g.n1, blocks = (uint64_t)g.nbx * g.nby;
+    auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
+    char *p = static_cast<char *>(mem);
+    BatchLat d{};
+    d.g = g;
+    d.spins = reinterpret_cast<uint8_t *>(p); p += al(n);
+    d.labels = reinterpret_cast<uint32_t *>(p); p += al(4 * n);
+    d.rng_state = reinterpret_cast<uint32_t *>(p); p += al(4 * tiles * b->W);
+    d.rng_sel = reinterpret_cast<uint8_t *>(p); p += al(tiles * b->W);
+    d.rng_iter = reinterpret_cast<uint32_t *>(p); p += al(4 * tiles);
+    d.edge = reinterpret_cast<uint32_t *>(p); p += al(4 * kEdgeWords * blocks);
+    d.obs = reinterpret_cast<Obs *>(p); p += al(sizeof(Obs));
+    d.series = reinterpret_cast<long long *>(p);
+    d.series_cap = b->series_cap;
+    d.p_add = swb_p_add(temperature);
+    d.sweeps_left = kUnlimited;
+    d.measure_every = 0;
+    d.chunks_left = lattice_chunks(g);
+    SWB_CUDA(cudaMemsetAsync(d.spins, 0, n, b->stream));
+    SWB_CUDA(cudaMemsetAsync(d.obs, 0, sizeof(Obs), b->stream));
+    switch (b->W) {
+    case 8: kb_rng_init<8><<<(unsigned)((tiles + 127) / 128), 128, 0, b->stream>>>((uint32_t)tiles, seed_base, d.rng_state, d.rng_sel, d.rng_iter); break;
+    case 16: kb_rng_init<16><<<(unsigned)((tiles + 127) / 128), 128, 0, b->stream>>>((uint32_t)tiles, seed_base, d.rng_state, d.rng_sel, d.rng_iter); break;
+    default: kb_rng_init<32><<<(unsigned)((tiles + 127) / 128), 128, 0, b->stream>>>((uint32_t)tiles, seed_base, d.rng_state, d.rng_sel, d.rng_iter); break;
+    }
+    SWB_LAUNCHED();
+    h.used = true;
+    h.d = d;
+    h.bytes = bytes;
+    h.mem = mem;
+    b->used += bytes;
+    b->lists_dirty = true;
+    if (int rc = upload_descriptor(b, slot))
+        return rc;
+    *id = slot;
+    return SWB_OK;
+}
+
+int swb_batch_remove(swb_batch *b, uint32_t id)
+{
+    HostLat *h = get_lat(b, id);
+    if (!h)
+        return fail(SWB_ERR_ARGUMENT, "no lattice %u", id);
+    if (int rc = bset_device(b))
+        return rc;
+    SWB_CUDA(cudaStreamSynchronize(b->stream));
+    SWB_CUDA(cudaFree(h->mem));
+    b->used -= h->bytes;
+    *h = HostLat{};
+    b->lists_dirty = true;
+    return SWB_OK;
+}
+
+int swb_batch_hot_start(swb_batch *b, uint32_t id, uint32_t seed)
+{
+    HostLat *h = get_lat(b, id);
+    if (!h)
+        return fail(SWB_ERR_ARGUMENT, "no lattice %u", id);
+    if (int rc = bset_device(b))
+        return rc;
+    const size_t n = (size_t)h->d.g.L0 * h->d.g.L1, chunks = (n + 63) / 64;
+    kb_hot_start<<<(unsigned)((chunks + 255) / 256), 256, 0, b->stream>>>(n, seed, h->d.spins);
+    SWB_LAUNCHED();
+    return SWB_OK;
+}
+
+int swb_batch_set_spins(swb_batch *b, uint32_t id, const uint8_t *host_spins)
+{
+    HostLat *h = get_lat(b, id);
+    if (!h || !host_spins)
+        return fail(SWB_ERR_ARGUMENT, "no lattice %u or NULL spins", id);
+    const size_t n = (size_t)h->d.g.L0 * h->d.g.L1;
+    for (size_t i = 0; i < n; ++i)
+        if (host_spins[i] > 1)
+            return fail(SWB_ERR_ARGUMENT, "spins must be 0 or 1");
+    if (int rc = bset_device(b))
+        return rc;
+    SWB_CUDA(cudaMemcpyAsync(h->d.spins, host_spins, n, cudaMemcpyHostToDevice, b->stream));
+    SWB_CUDA(cudaStreamSynchronize(b->stream));
+    return SWB_OK;
+}
+
+int swb_batch_get_spins(swb_batch *b, uint32_t id, uint8_t *host_spins)
+{
+    HostLat *h = get_lat(b, id);
+    if (!h || !host_spins)
+        return fail(SWB_ERR_ARGUMENT, "no lattice %u or NULL spins", id);
+    if (int rc = bset_device(b))
+        return rc;
+    SWB_CUDA(cudaMemcpyAsync(host_spins, h->d.spins, (size_t)h->d.g.L0 * h->d.g.L1, cudaMemcpyDeviceToHost, b->stream));
+    SWB_CUDA(cudaStreamSynchronize(b->stream));
+    return SWB_OK;
+}
+
+int swb_batch_set_temperature(swb_batch *b, uint32_t id, float temperature)
+{
+    HostLat *h = get_lat(b, id);
+    if (!h)
+        return fail(SWB_ERR_ARGUMENT, "no lattice %u", id);
+    if (!(temperature > 0.0f) || !std::isfinite(temperature))
+        return fail(SWB_ERR_ARGUMENT, "temperature must be positive and finite");
+    if (int rc = bset_device(b))
+        return rc;
+    h->d.p_add = swb_p_add(temperature);
+    SWB_CUDA(cudaMemcpyAsync(&b->d_lats[id].p_add, &h->d.p_add, sizeof(float), cudaMemcpyHostToDevice, b->stream));
+    SWB_CUDA(cudaStreamSynchronize(b->stream));
+    return SWB_OK;
+}
+
+int swb_batch_set_schedule(swb_batch *b, uint32_t id, uint32_t sweeps, uint32_t measure_every)
+{
+    HostLat *h = get_lat(b, id);
+    if (!h)
+        return fail(SWB_ERR_ARGUMENT, "no lattice %u", id);
+    if (int rc = bset_device(b))
+        return rc;
+    uint32_t v[2] = {sweeps, measure_every};
+    SWB_CUDA(cudaMemcpyAsync(&b->d_lats[id].sweeps_left, &v[0], 4, cudaMemcpyHostToDevice, b->stream));
+    SWB_CUDA(cudaMemcpyAsync(&b->d_lats[id].measure_every, &v[1], 4, cudaMemcpyHostToDevice, b->stream));
+    SWB_CUDA(cudaStreamSynchronize(b->stream));
+    h->d.sweeps_left = sweeps;
+    h->d.measure_every = measure_every;
+    return SWB_OK;
+}
+
+int swb_batch_status(swb_batch *b, uint32_t id, uint32_t *sweeps_left, uint32_t *sweeps_done)
+{
+    HostLat *h = get_lat(b, id);
+    if (!h)
+        return fail(SWB_ERR_ARGUMENT, "no lattice %u", id);
+    if (int rc = bset_device(b))
+        return rc;
+    BatchLat d;
+    SWB_CUDA(cudaMemcpyAsync(&d, b->d_lats + id, sizeof(d), cudaMemcpyDeviceToHost, b->stream));
+    SWB_CUDA(cudaStreamSynchronize(b->stream));
+    if (sweeps_left) *sweeps_left = d.sweeps_left;
+    if (sweeps_done) *sweeps_done = d.sweeps_done;
+    return SWB_OK;
+}
+
+int swb_batch_sweep(swb_batch *b, uint32_t n_rounds, int measure)
+{
+    if (!b)
+        return fail(SWB_ERR_ARGUMENT, "NULL handle");
+    if (int rc = bset_device(b))
+        return rc;
+    return rounds(b, n_rounds, measure != 0);
+}
+
+int swb_batch_synchronize(swb_batch *b)
+{
+    if (!b)
+        return fail(SWB_ERR_ARGUMENT, "NULL handle");
+    if (int rc = bset_device(b))
+        return rc;
+    SWB_CUDA(cudaStreamSynchronize(b->stream));
+    return SWB_OK;
+}
+
+int swb_batch_sweep_timed(swb_batch *b, uint32_t n_rounds, int per_kernel, float *ms)
+{
+    if (!b || !ms)
+        return fail(SWB_ERR_ARGUMENT, "NULL argument");
+    if (int rc = bset_device(b))
+        return rc;
+    if (int rc = rebuild_lists(b))
+        return rc;
+    ms[0] = ms[1] = ms[2] = ms[3] = 0.0f;
+    cudaEvent_t ev[5];
+    for (auto &e : ev)
+        SWB_CUDA(cudaEventCreate(&e));
+    SWB_CUDA(cudaEventRecord(ev[0], b->stream));
+    int rc = SWB_OK;
+    if (!per_kernel) {
+        rc = rounds(b, n_rounds, false);
+    } else {
+        for (uint32_t r = 0; r < n_rounds && !rc; ++r) {
+            kb_begin_round<<<4, 128, 0, b->stream>>>(b->d_lats, b->d_active, b->d_ctr);
+            SWB_LAUNCHED();
+            SWB_CUDA(cudaEventRecord(ev[1], b->stream));
+            switch (b->W) {
+            case 8: kb_assign<8><<<b->grid_assign, kBatchThreads, b->smem_assign, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix, b->d_ctr); break;
+            case 16: kb_assign<16><<<b->grid_assign, kBatchThreads, b->smem_assign, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix, b->d_ctr); break;
+            default: kb_assign<32><<<b->grid_assign, kBatchThreads, b->smem_assign, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix, b->d_ctr); break;
+            }
+            SWB_LAUNCHED();
+            SWB_CUDA(cudaEventRecord(ev[2], b->stream));
+            kb_merge<<<b->grid_other, kBatchThreads, 0, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix, b->d_ctr);
+            SWB_LAUNCHED();
+            SWB_CUDA(cudaEventRecord(ev[3], b->stream));
+            kb_flip<<<b->grid_other, kBatchThreads, 0, b->stream>>>(b->d_lats, b->d_active, b->d_chunk_prefix, b->d_ctr);
+            SWB_LAUNCHED();
+            SWB_CUDA(cudaEventRecord(ev[4], b->stream));
+            SWB_CUDA(cudaEventSynchronize(ev[4]));
+            float t;
+            SWB_CUDA(cudaEventElapsedTime(&t, ev[1], ev[2]));
+            ms[1] += t;
+            SWB_CUDA(cudaEventElapsedTime(&t, ev[2], ev[3]));
+            ms[2] += t;
+            SWB_CUDA(cudaEventElapsedTime(&t, ev[3], ev[4]));
+            ms[3] += t;
+        }
+    }
+    SWB_CUDA(cudaEventRecord(ev[4], b->stream));
+    SWB_CUDA(cudaEventSynchronize(ev[4]));
+    SWB_CUDA(cudaEventElapsedTime(&ms[0], ev[0], ev[4]));
+    for (auto &e : ev)
+        cudaEventDestroy(e);
+    return rc;
+}
+
+int swb_batch_accumulators(swb_batch *b, uint32_t id, double *out)
+{
+    HostLat *h = get_lat(b, id);
+    if (!h || !out)
+        return fail(SWB_ERR_ARGUMENT, "no lattice %u or NULL out", id);
+    if (int rc = bset_device(b))
+        return rc;
+    Obs o;
+    SWB_CUDA(cudaMemcpyAsync(&o, h->d.obs, sizeof(o), cudaMemcpyDeviceToHost, b->stream));
+    SWB_CUDA(cudaStreamSynchronize(b->stream));
+    std::memcpy(out, o.acc, sizeof(o.acc));
+    return SWB_OK;
+}
+
+int swb_batch_samples(swb_batch *b, uint32_t id, int64_t *em, uint64_t capacity, uint64_t *count)
+{
+    HostLat *h = get_lat(b, id);
+    if (!h || !count)
+        return fail(SWB_ERR_ARGUMENT, "no lattice %u or NULL count", id);
+    if (int rc = bset_device(b))
+        return rc;
+    Obs o;
+    SWB_CUDA(cudaMemcpyAsync(&o, h->d.obs, sizeof(o), cudaMemcpyDeviceToHost, b->stream));
+    SWB_CUDA(cudaStreamSynchronize(b->stream));
+    *count = o.n_samples;
+    if (o.n_samples > h->d.series_cap)
+        return fail(SWB_ERR_CAPACITY, "%llu samples recorded, series keeps %llu", o.n_samples, h->d.series_cap);
+    const uint64_t k = std::min<uint64_t>(o.n_samples, capacity);
+    if (k && em) {
+        SWB_CUDA(cudaMemcpyAsync(em, h->d.series, k * 16, cudaMemcpyDeviceToHost, b->stream));
+        SWB_CUDA(cudaStreamSynchronize(b->stream));
+    }
+    return SWB_OK;
+}
+
+int swb_batch_get_rng(swb_batch *b, uint32_t id, uint32_t *state, uint32_t *a, uint32_t *c, uint32_t *iteration)
+{
+    HostLat *h = get_lat(b, id);
+    if (!h || !state || !a || !c || !iteration)
+        return fail(SWB_ERR_ARGUMENT, "no lattice %u or NULL argument", id);
+    if (int rc = bset_device(b))
+        return rc;
+    const size_t tiles = (size_t)h->d.g.n0 * h->d.g.n1, nw = tiles * b->W;
+    std::vector<uint8_t> sel(nw);
+    SWB_CUDA(cudaMemcpyAsync(state, h->d.rng_state, nw * 4, cudaMemcpyDeviceToHost, b->stream));
+    SWB_CUDA(cudaMemcpyAsync(sel.data(), h->d.rng_sel, nw, cudaMemcpyDeviceToHost, b->stream));
+    SWB_CUDA(cudaMemcpyAsync(iteration, h->d.rng_iter, tiles * 4, cudaMemcpyDeviceToHost, b->stream));
+    SWB_CUDA(cudaStreamSynchronize(b->stream));
+    for (size_t i = 0; i < nw; ++i) {
+        a[i] = lcg_param_a(sel[i]);
+        c[i] = lcg_param_c(sel[i]);
+    }
+    return SWB_OK;
+}
+
+int swb_batch_info(swb_batch *b, uint32_t id, uint32_t *geometry)
+{
+    HostLat *h = get_lat(b, id);
+    if (!h || !geometry)
+        return fail(SWB_ERR_ARGUMENT, "no lattice %u or NULL argument", id);
+    const Geo &g = h->d.g;
+    const uint32_t v[8] = {g.L0, g.L1, g.TX, g.TY, g.TBX, g.TBY, g.n0 * g.n1, g.nbx * g.nby};
+    std::memcpy(geometry, v, sizeof(v));
+    return SWB_OK;
+}
+
+int swb_batch_memory(swb_batch *b, uint64_t *used, uint64_t *budget)
+{
+    if (!b)
+        return fail(SWB_ERR_ARGUMENT, "NULL handle");
+    if (used) *used = b->used;
+    if (budget) *budget = b->budget;
+    return SWB_OK;
+}
+
+int swb_batch_update_host(swb_batch *b, uint32_t count, const uint32_t *ids, const uint8_t *const *spins_in,
+                          uint8_t *const *spins_out)
+{
+    if (!b || (count && (!ids || !spins_in || !spins_out)))
+        return fail(SWB_ERR_ARGUMENT, "NULL argument");
+    if (int rc = bset_device(b))
+        return rc;
+    for (uint32_t k = 0; k < count; ++k) {
+        HostLat *h = get_lat(b, ids[k]);
+        if (!h)
+            return fail(SWB_ERR_ARGUMENT, "no lattice %u", ids[k]);
+        SWB_CUDA(cudaMemcpyAsync(h->d.spins, spins_in[k], (size_t)h->d.g.L0 * h->d.g.L1, cudaMemcpyHostToDevice,
+                                 b->stream));
+    }
+    if (int rc = rounds(b, 1, false))
+        return rc;
+    for (uint32_t k = 0; k < count; ++k) {
+        HostLat *h = get_lat(b, ids[k]);
+        SWB_CUDA(cudaMemcpyAsync(spins_out[k], h->d.spins, (size_t)h->d.g.L0 * h->d.g.L1, cudaMemcpyDeviceToHost,
+                                 b->stream));
+    }
+    SWB_CUDA(cudaStreamSynchronize(b->stream));
+    return SWB_OK;
+}
+
+}  // extern "C"

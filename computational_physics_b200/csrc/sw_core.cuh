@@ -1,0 +1,376 @@
+// Shared device code of the Swendsen-Wang engine: lattice geometry, the per-block assign
+// phase (lcg32 draws, bonds, shared-memory union-find) and the per-block edge merge.  Used by
+// the single-lattice kernels (sw_plain.cu) and the batched persistent kernels (sw_batch.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <string>
+
+#include "../../include/swb200.h"
+#include "sw_device.cuh"
+
+namespace swb {
+
+// ------------------------------------------------------------------------------------------
+// errors and launch accounting (defined in sw_plain.cu)
+
+extern thread_local std::string g_last_error;
+extern std::atomic<uint64_t> g_launches;
+int fail(int code, const char *fmt, ...);
+
+#define SWB_CUDA(call)                                                                          \
+    do {                                                                                        \
+        cudaError_t err__ = (call);                                                             \
+        if (err__ != cudaSuccess)                                                               \
+            return ::swb::fail(SWB_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(err__)); \
+    } while (0)
+
+#define SWB_LAUNCHED()                                                                           \
+    do {                                                                                         \
+        ::swb::g_launches.fetch_add(1, std::memory_order_relaxed);                               \
+        cudaError_t err__ = cudaGetLastError();                                                  \
+        if (err__ != cudaSuccess)                                                                \
+            return ::swb::fail(SWB_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(err__)); \
+    } while (0)
+
+// ------------------------------------------------------------------------------------------
+// geometry
+
+struct Geo {
+    uint32_t L0, L1;    // extent
+    uint32_t TX, TY;    // tile
+    uint32_t TBX, TBY;  // tiles per block
+    uint32_t BX, BY;    // block in sites
+    uint32_t n0, n1;    // tiles per direction
+    uint32_t nbx, nby;  // blocks per direction
+};
+
+// Tiles per block: blocks of up to 128 x 32 sites, at most 1024 threads (one per lcg lane).
+// tbx / tby (tiles per block) of 0 pick the largest block within 128 x 32 sites and
+// max_threads threads; explicit values are clamped to those limits.
+inline Geo make_geo(uint32_t L0, uint32_t L1, uint32_t TX, uint32_t TY, uint32_t W, uint32_t max_threads = 1024,
+                    uint32_t tbx = 0, uint32_t tby = 0)
+{
+    Geo g{};
+    g.L0 = L0; g.L1 = L1; g.TX = TX; g.TY = TY;
+    g.n0 = (L0 + TX - 1) / TX;
+    g.n1 = (L1 + TY - 1) / TY;
+    g.TBX = 128 / TX;
+    g.TBY = TY >= 32 ? 1 : 32 / TY;
+    if (tbx && tbx < g.TBX)
+        g.TBX = tbx;
+    if (tby && tby < g.TBY)
+        g.TBY = tby;
+    while (g.TBX * g.TBY * W > max_threads && g.TBY > 1)
+        g.TBY /= 2;
+    while (g.TBX * g.TBY * W > max_threads && g.TBX > 1)
+        g.TBX /= 2;
+    // Do not make blocks larger than the lattice needs.
+    while (g.TBX > 1 && (g.TBX / 2) * TX >= L0)
+        g.TBX /= 2;
+    while (g.TBY > 1 && (g.TBY / 2) * TY >= L1)
+        g.TBY /= 2;
+    g.BX = g.TBX * TX;
+    g.BY = g.TBY * TY;
+    g.nbx = (L0 + g.BX - 1) / g.BX;
+    g.nby = (L1 + g.BY - 1) / g.BY;
+    return g;
+}
+
+constexpr uint32_t kEdgeWords = 8;  // per block: [0] right edge rows, [1..4] bottom edge columns
+
+struct AssignSmem {
+    uint32_t parent, accM, accX, accY, edge, bond, sp, total, pitch;
+};
+
+__host__ __device__ inline AssignSmem assign_smem(const Geo &g)
+{
+    AssignSmem s{};
+    const uint32_t ns = g.BX * g.BY, ntb = g.TBX * g.TBY;
+    s.pitch = g.BX + 4;
+    s.parent = 0;
+    s.accM = s.parent + ns * 4;
+    s.accX = s.accM + ntb * 8;
+    s.accY = s.accX + ntb * g.TY * 4;
+    s.edge = s.accY + ntb * g.TY * 4;
+    s.bond = s.edge + kEdgeWords * 4;
+    s.sp = s.bond + ns;
+    s.total = s.sp + (g.BY + 1) * s.pitch;
+    s.total = (s.total + 15) & ~15u;
+    return s;
+}
+
+// ------------------------------------------------------------------------------------------
+// kernels
+
+// Device buffers of one lattice.
+struct LatView {
+    Geo g;
+    uint8_t *spins;
+    uint32_t *labels;
+    uint32_t *rng_state;
+    uint8_t *rng_sel;
+    uint32_t *rng_iter;
+    uint32_t *edge;
+    float p_add;
+};
+
+// Block (bxi, byi) of a lattice: lcg32 draws, bonds, union-find in shared memory.  Runs on
+// all threads of the CTA (at least TBX * TBY * W of them); smem holds assign_smem(g).total bytes.
+template <int W>
+__device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, const uint32_t byi,
+                                             const uint8_t *__restrict__ spins, uint32_t *__restrict__ labels,
+                                             uint32_t *__restrict__ rng_state, uint8_t *__restrict__ rng_sel,
+                                             uint32_t *__restrict__ rng_iter, const float p_add,
+                                             uint32_t *__restrict__ edge, uint8_t *__restrict__ dbg_bonds,
+                                             uint32_t *__restrict__ dbg_assign, unsigned char *smem)
+{
+    const AssignSmem L = assign_smem(g);
+    uint32_t *parent = reinterpret_cast<uint32_t *>(smem + L.parent);
+    uint64_t *accM = reinterpret_cast<uint64_t *>(smem + L.accM);
+    uint32_t *accX = reinterpret_cast<uint32_t *>(smem + L.accX);
+    uint32_t *accY = reinterpret_cast<uint32_t *>(smem + L.accY);
+    uint32_t *edge_s = reinterpret_cast<uint32_t *>(smem + L.edge);
+    uint8_t *bond = smem + L.bond;
+    uint8_t *sp = smem + L.sp;
+
+    const uint32_t tid = threadIdx.x, nthr = blockDim.x;
+    const uint32_t BX = g.BX, BY = g.BY, NS = BX * BY, ntb = g.TBX * g.TBY;
+    const uint32_t x0 = bxi * BX, y0 = byi * BY;
+    const uint32_t bxv = min(BX, g.L0 - x0), byv = min(BY, g.L1 - y0);
+    const uint32_t pitch = L.pitch;
+
+    for (uint32_t i = tid; i < ntb * g.TY * 2 + kEdgeWords; i += nthr)
+        accX[i] = 0;  // accX, accY and edge_s are contiguous
+
+    // ---- 1. spins of the block and its halo (column x0+bxv and row y0+byv, periodic)
+    {
+        const uint32_t warp = tid >> 5, lane32 = tid & 31, nwarps = nthr >> 5;
+        const uint32_t hx = (x0 + bxv) % g.L0, hy = (y0 + byv) % g.L1;
+        const bool words = (g.L0 % 4) == 0;
+        for (uint32_t yl = warp; yl <= byv; yl += nwarps) {
+            const uint32_t gy = yl < byv ? y0 + yl : hy;
+            const uint8_t *row = spins + (size_t)gy * g.L0 + x0;
+            uint8_t *dst = sp + yl * pitch;
+            if (words) {
+                for (uint32_t w = lane32; w * 4 < bxv; w += 32)
+                    *reinterpret_cast<uint32_t *>(dst + 4 * w) = __ldg(reinterpret_cast<const uint32_t *>(row) + w);
+            } else {
+                for (uint32_t x = lane32; x < bxv; x += 32)
+                    dst[x] = __ldg(row + x);
+            }
+        }
+        for (uint32_t yl = tid; yl < byv; yl += nthr)
+            sp[yl * pitch + bxv] = __ldg(spins + (size_t)(y0 + yl) * g.L0 + hx);
+    }
+    __syncthreads();
+
+    // ---- 2. lcg32 draws of this sweep, one W-lane segment per tile
+    {
+        const uint32_t tb = tid / W, lane = tid % W;
+        const uint32_t tgx = bxi * g.TBX + tb % g.TBX, tgy = byi * g.TBY + tb / g.TBX;
+        const bool on = tb < ntb && tgx < g.n0 && tgy < g.n1;
+        const uint32_t tile = tgy * g.n0 + tgx;
+        const uint32_t jjmax = on ? min(g.TY, g.L1 - tgy * g.TY) : 0;
+        uint32_t st = 0, sel = 0, it = 0;
+        if (on) {
+            st = rng_state[(size_t)tile * W + lane];
+            sel = rng_sel[(size_t)tile * W + lane];
+            it = rng_iter[tile];
+        }
+        uint32_t a = lcg_param_a(sel), c = lcg_param_c(sel);
+        const uint32_t Ur = (g.TX + W - 1) / W, Um = (g.TX + g.TY + W - 1) / W;
+        const uint32_t nrow = on ? 2 * jjmax - 1 : 0;
+        const uint32_t rowU = nrow * Ur, myU = on ? rowU + Um : 0;
+        const uint32_t maxU = (2 * g.TY - 1) * Ur + Um;
+        const uint32_t seg_shift = ((tid & 31) / W) * W;
+        uint64_t mbits = 0;
+        for (uint32_t u = 0; u < maxU; ++u) {
+            const bool upd = u < myU;
+            const uint32_t itn = it + 1;
+            const bool rot = upd && (itn % kShuffleDistance) == 0;
+            if (__any_sync(0xffffffffu, rot)) {
+                // Parameter rotation of random/src/lcg32.cpp:168-188: lane i takes the pair of
+                // lane (i + state[it & (W-1)] + (it odd ? 0 : 1)) & (W-1), before stepping.
+                const uint32_t src = __shfl_sync(0xffffffffu, st, itn & (W - 1), W);
+                const uint32_t from = (lane + src + ((itn & 1u) ? 0u : 1u)) & (W - 1);
+                const uint32_t a2 = __shfl_sync(0xffffffffu, a, from, W);
+                const uint32_t c2 = __shfl_sync(0xffffffffu, c, from, W);
+                const uint32_t s2 = __shfl_sync(0xffffffffu, sel, from, W);
+                if (rot) {
+                    a = a2;
+                    c = c2;
+                    sel = s2;
+                }
+            }
+            bool bit = false, is_row = false;
+            uint32_t req = 0, sub = 0;
+            if (upd) {
+                it = itn;
+                st = a * st + c;
+                if (u < rowU) {
+                    req = u / Ur;
+                    sub = u - req * Ur;
+                    is_row = true;
+                    bit = sub * W + lane < g.TX && lcg_accept(st, p_add);
+                } else {
+                    sub = u - rowU;
+                    bit = sub * W + lane < g.TX + g.TY && lcg_accept(st, p_add);
+                }
+            }
+            const uint32_t m = __ballot_sync(0xffffffffu, bit);
+            const uint32_t seg = (W == 32) ? m : ((m >> seg_shift) & ((1u << (W & 31)) - 1u));
+            if (lane == 0 && upd) {
+                if (is_row) {
+                    const uint32_t word = seg << (sub * W);
+                    if (req < jjmax)
+                        accX[tb * g.TY + req] |= word;
+                    else
+                        accY[tb * g.TY + req - jjmax] |= word;
+                } else {
+                    mbits |= (uint64_t)seg << (sub * W);
+                }
+            }
+        }
+        if (on) {
+            rng_state[(size_t)tile * W + lane] = st;
+            rng_sel[(size_t)tile * W + lane] = (uint8_t)sel;
+            if (lane == 0)
+                rng_iter[tile] = it;
+        }
+        if (lane == 0 && tb < ntb)
+            accM[tb] = mbits;
+    }
+    __syncthreads();
+
+    // ---- 3. bonds (bit 0 +x, bit 1 +y): equal spins and an accepted draw.  The last
+    // column / row of a tile bonds through the merge draw: [0, TX) bottom, [TX, TX+TY) right.
+    for (uint32_t l = tid; l < NS; l += nthr) {
+        const uint32_t xl = l % BX, yl = l / BX;
+        uint8_t b = 0;
+        if (xl < bxv && yl < byv) {
+            const uint32_t tbx = xl / g.TX, tby = yl / g.TY, tb = tby * g.TBX + tbx;
+            const uint32_t ii = xl - tbx * g.TX, jj = yl - tby * g.TY;
+            const uint32_t iimax = min(g.TX, bxv - tbx * g.TX), jjmax = min(g.TY, byv - tby * g.TY);
+            const uint8_t s = sp[yl * pitch + xl];
+            const uint32_t xa = (ii + 1 < iimax) ? (accX[tb * g.TY + jj] >> ii) : (uint32_t)(accM[tb] >> (g.TX + jj));
+            const uint32_t ya = (jj + 1 < jjmax) ? (accY[tb * g.TY + jj] >> ii) : (uint32_t)(accM[tb] >> ii);
+            b = (uint8_t)(((xa & 1u) && s == sp[yl * pitch + xl + 1]) | (((ya & 1u) && s == sp[(yl + 1) * pitch + xl]) << 1));
+        }
+        bond[l] = b;
+        parent[l] = l;
+    }
+    __syncthreads();
+
+    // ---- 4. tile-local components (the reference's AssignLabels result)
+    for (uint32_t l = tid; l < NS; l += nthr) {
+        const uint8_t b = bond[l];
+        if (!b)
+            continue;
+        const uint32_t xl = l % BX, yl = l / BX;
+        const uint32_t tbx = xl / g.TX, tby = yl / g.TY;
+        const uint32_t ii = xl - tbx * g.TX, jj = yl - tby * g.TY;
+        const uint32_t iimax = min(g.TX, bxv - tbx * g.TX), jjmax = min(g.TY, byv - tby * g.TY);
+        if ((b & 1) && ii + 1 < iimax)
+            uf_union(parent, l, l + 1);
+        if ((b & 2) && jj + 1 < jjmax)
+            uf_union(parent, l, l + BX);
+    }
+    __syncthreads();
+    if (dbg_assign != nullptr) {
+        for (uint32_t l = tid; l < NS; l += nthr) {
+            const uint32_t xl = l % BX, yl = l / BX;
+            if (xl < bxv && yl < byv) {
+                const uint32_t r = uf_find(parent, l);
+                const size_t site = (size_t)(y0 + yl) * g.L0 + x0 + xl;
+                dbg_assign[site] = (y0 + r / BX) * g.L0 + x0 + r % BX;
+                dbg_bonds[site] = bond[l];
+            }
+        }
+        __syncthreads();
+    }
+
+    // ---- 5. bonds between tiles of this block; bonds leaving the block go to k_merge
+    for (uint32_t l = tid; l < NS; l += nthr) {
+        const uint8_t b = bond[l];
+        if (!b)
+            continue;
+        const uint32_t xl = l % BX, yl = l / BX;
+        const uint32_t tbx = xl / g.TX, tby = yl / g.TY;
+        const uint32_t ii = xl - tbx * g.TX, jj = yl - tby * g.TY;
+        const uint32_t iimax = min(g.TX, bxv - tbx * g.TX), jjmax = min(g.TY, byv - tby * g.TY);
+        if ((b & 1) && ii + 1 == iimax) {
+            if (xl + 1 < bxv)
+                uf_union(parent, l, l + 1);
+            else
+                atomicOr(edge_s, 1u << yl);
+        }
+        if ((b & 2) && jj + 1 == jjmax) {
+            if (yl + 1 < byv)
+                uf_union(parent, l, l + BX);
+            else
+                atomicOr(edge_s + 1 + (xl >> 5), 1u << (xl & 31));
+        }
+    }
+    __syncthreads();
+
+    // ---- 6. block-local minimum as a global site index
+    for (uint32_t l = tid; l < NS; l += nthr) {
+        const uint32_t xl = l % BX, yl = l / BX;
+        if (xl < bxv && yl < byv) {
+            const uint32_t r = uf_find(parent, l);
+            labels[(size_t)(y0 + yl) * g.L0 + x0 + xl] = (y0 + r / BX) * g.L0 + x0 + r % BX;
+        }
+    }
+    if (tid < kEdgeWords)
+        edge[((size_t)byi * g.nbx + bxi) * kEdgeWords + tid] = edge_s[tid];
+}
+
+// Unions across the right and bottom edge (periodic) of block blk: thread t < BY takes row
+// t of the right edge, BY <= t < BY + BX column t - BY of the bottom edge.
+__device__ __forceinline__ void merge_block(const Geo &g, const uint32_t blk, const uint32_t t,
+                                            const uint32_t *__restrict__ edge, uint32_t *labels)
+{
+    const uint32_t bxi = blk % g.nbx, byi = blk / g.nbx;
+    const uint32_t x0 = bxi * g.BX, y0 = byi * g.BY;
+    const uint32_t bxv = min(g.BX, g.L0 - x0), byv = min(g.BY, g.L1 - y0);
+    const uint32_t *e = edge + (size_t)blk * kEdgeWords;
+    size_t s = 0, nb = 0;
+    bool go = false;
+    if (t < g.BY) {
+        if (t < byv && ((e[0] >> t) & 1u)) {
+            s = (size_t)(y0 + t) * g.L0 + x0 + bxv - 1;
+            nb = (size_t)(y0 + t) * g.L0 + (x0 + bxv) % g.L0;
+            go = true;
+        }
+    } else {
+        const uint32_t xl = t - g.BY;
+        if (xl < bxv && ((e[1 + (xl >> 5)] >> (xl & 31)) & 1u)) {
+            s = (size_t)(y0 + byv - 1) * g.L0 + x0 + xl;
+            nb = (size_t)((y0 + byv) % g.L1) * g.L0 + x0 + xl;
+            go = true;
+        }
+    }
+    if (go) {
+        const volatile uint32_t *vl = labels;
+        const uint32_t a = vl[s], b = vl[nb];
+        if (a != b)
+            uf_union(labels, a, b);
+    }
+}
+
+// Observables.  Per-sweep integer sums land in obs->e / obs->m; the last CTA turns them into
+// E/N, M/N, accumulates E, E^2, |M| in FP64 and appends (e, m) to the sample series.
+struct Obs {
+    unsigned long long e, m;       // running int64 sums (two's complement) of this measurement
+    unsigned int done;             // CTAs finished
+    unsigned int pad;
+    long long last_e, last_m;      // sums of the last measurement
+    double acc[4];                 // sum E/N, sum (E/N)^2, sum |M/N|, samples
+    unsigned long long n_samples;  // samples recorded (may exceed capacity)
+};
+
+}  // namespace swb

@@ -1,0 +1,103 @@
+// Device building blocks of the Swendsen-Wang engine (sm_100a).
+//
+//  * lcg32 lanes in registers: one thread holds one lane of a tile's stream; a tile's W
+//    lanes sit in one W-wide segment of a warp, so the reference's periodic parameter
+//    rotation (random/src/lcg32.cpp:162-195) is a segment-local __shfl_sync.
+//  * drand48 with jump-ahead, for the bit-exact hot start and stream seeding.
+//  * lock-free union-find toward the minimum index (shared or global memory), the
+//    reference's atomic-min equivalence rule (ising/src/swendsen_wang_cpu.cpp:107-156).
+#pragma once
+
+#include <cstdint>
+
+namespace swb {
+
+// The five Numerical Recipes (a, c) pairs of random/src/lcg32.cpp:128-135, by index.
+__host__ __device__ __forceinline__ uint32_t lcg_param_a(uint32_t sel)
+{
+    return sel == 0 ? 1372383749u : sel == 1 ? 2891336453u : sel == 2 ? 2024337845u : sel == 3 ? 32310901u : 29943829u;
+}
+__host__ __device__ __forceinline__ uint32_t lcg_param_c(uint32_t sel)
+{
+    return sel == 0 ? 1289706101u : sel == 1 ? 1640531513u : sel == 2 ? 797082193u : sel == 3 ? 626627237u : 1013904223u;
+}
+
+constexpr uint32_t kShuffleDistance = 15;          // LCG32_State::ShuffleDistance (lcg32.hpp:43)
+constexpr float kTwoPowMinus32 = 2.3283064365386963e-10f;  // the float the reference's literal rounds to
+
+// Accept test of the bond draw: (float)u * 2^-32 < p_add with u rounded to nearest
+// (random/src/lcg32.cpp:231-240 and the '< p_add' of the callers).
+__device__ __forceinline__ bool lcg_accept(uint32_t u, float p_add)
+{
+    return __fmul_rn(__uint2float_rn(u), kTwoPowMinus32) < p_add;
+}
+
+// ---- drand48: X' = 0x5DEECE66D X + 0xB mod 2^48 (POSIX), used by LCG32_State::Init and the
+// Lattice<2> hot start.
+constexpr uint64_t kDrandA = 0x5DEECE66Dull;
+constexpr uint64_t kDrandC = 0xBull;
+constexpr uint64_t kDrandMask = (1ull << 48) - 1;
+
+__host__ __device__ __forceinline__ uint64_t drand48_seed(uint32_t seed)
+{
+    return ((uint64_t)seed << 16) | 0x330Eull;
+}
+__host__ __device__ __forceinline__ uint64_t drand48_step(uint64_t x)
+{
+    return (kDrandA * x + kDrandC) & kDrandMask;
+}
+// drand48() as a double: X * 2^-48 exactly.
+__host__ __device__ __forceinline__ double drand48_value(uint64_t x)
+{
+    return (double)x * 0x1p-48;  // exact: x < 2^48
+}
+// Affine map of k drand48 steps: X_k = A X + C (mod 2^48).
+__host__ __device__ inline void drand48_jump(uint64_t k, uint64_t &A, uint64_t &C)
+{
+    uint64_t a = kDrandA, c = kDrandC;
+    A = 1;
+    C = 0;
+    while (k) {
+        if (k & 1) {
+            C = (a * C + c) & kDrandMask;
+            A = (a * A) & kDrandMask;
+        }
+        c = (a * c + c) & kDrandMask;
+        a = (a * a) & kDrandMask;
+        k >>= 1;
+    }
+}
+
+// ---- union-find toward the minimum index.  After all unions every set's root is its
+// smallest member, which is the canonical label.
+__device__ __forceinline__ uint32_t uf_find(const volatile uint32_t *p, uint32_t x)
+{
+    uint32_t y = p[x];
+    while (y != x) {
+        x = y;
+        y = p[x];
+    }
+    return x;
+}
+
+__device__ __forceinline__ void uf_union(uint32_t *p, uint32_t a, uint32_t b)
+{
+    const volatile uint32_t *vp = p;
+    while (true) {
+        a = uf_find(vp, a);
+        b = uf_find(vp, b);
+        if (a == b)
+            return;
+        if (a > b) {
+            const uint32_t t = a;
+            a = b;
+            b = t;
+        }
+        const uint32_t old = atomicMin(p + b, a);
+        if (old == b)
+            return;  // b was a root and now hangs below a
+        b = old;     // b was re-linked meanwhile: join a with b's new parent
+    }
+}
+
+}  // namespace swb

@@ -1,0 +1,778 @@
+// Swendsen-Wang sweep for the 2D Ising model on one B200 (sm_100a), behind the C ABI of
+// include/swb200.h.
+//
+// One sweep = three kernels on the handle's stream (reference phases in brackets,
+// ising/src/swendsen_wang.cpp:201-219):
+//
+//   k_assign  [AssignLabels + the in-block part of MergeLabels]  one CTA per block of
+//             TBX x TBY tiles.  Each tile's lcg32 stream lives in the registers of one
+//             W-lane warp segment; the bond draws become bit masks via __ballot_sync.
+//             Spins of the block plus a one-site halo are staged in shared memory, bonds
+//             are formed, and a lock-free union-find toward the minimum index labels the
+//             block in shared memory (tile-local bonds first -- the reference's
+//             AssignLabels result -- then the bonds between tiles of the block).  Writes
+//             each site's block-local minimum global index and the bond bits of the
+//             block's right and bottom edge.
+//   k_merge   [MergeLabels across blocks]  atomicMin union on the global label array for
+//             the edge bonds recorded by k_assign.
+//   k_flip    [ResolveLabels + FlipClusters]  pointer chase to the root (the cluster's
+//             minimum site index) and spin ^= root & 1.
+//
+// k_measure (every measure_every-th sweep) reduces energy and magnetisation on the device
+// and accumulates E, E^2, |M| in FP64 (Lattice<2>::GetEnergyAndMagnetization,
+// ising/src/lattice.cpp:127-165, and the sums of ising/src/ising_2d.cpp:127-146).
+//
+// Bit-exactness with the reference CPU path: the stream of tile t is seeded seed_base + t
+// and consumed in the reference's order (rows' x-draws, rows' y-draws, then the merge draw
+// of tx + ty numbers), the float threshold is evaluated exactly as the reference does, and
+// labels are canonical (minimum site index), so bonds, labels and flipped spins match.
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/swb200.h"
+#include "sw_core.cuh"
+
+namespace swb {
+
+// ------------------------------------------------------------------------------------------
+// errors and launch accounting
+
+thread_local std::string g_last_error;
+std::atomic<uint64_t> g_launches{0};
+
+int fail(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+template <int W>
+__global__ void __launch_bounds__(1024) k_assign(const Geo g, const uint8_t *__restrict__ spins,
+                                                 uint32_t *__restrict__ labels, uint32_t *__restrict__ rng_state,
+                                                 uint8_t *__restrict__ rng_sel, uint32_t *__restrict__ rng_iter,
+                                                 const float p_add, uint32_t *__restrict__ edge,
+                                                 uint8_t *__restrict__ dbg_bonds, uint32_t *__restrict__ dbg_assign)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    assign_block<W>(g, blockIdx.x, blockIdx.y, spins, labels, rng_state, rng_sel, rng_iter, p_add, edge, dbg_bonds,
+                    dbg_assign, smem);
+}
+
+__global__ void __launch_bounds__(256) k_merge(const Geo g, const uint32_t *__restrict__ edge, uint32_t *labels)
+{
+    merge_block(g, blockIdx.x, threadIdx.x, edge, labels);
+}
+
+// Root of each site's label chain; spin ^= root & 1.  Optionally writes the root back
+// (the reference's ResolveLabels result).
+template <bool kWriteLabels>
+__global__ void __launch_bounds__(256) k_flip(const uint32_t n, uint8_t *__restrict__ spins, uint32_t *labels)
+{
+    const volatile uint32_t *vl = labels;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    if ((n & 3u) == 0) {
+        const size_t nq = n >> 2;
+        for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += stride) {
+            uint4 lab;
+            if (kWriteLabels) {
+                lab.x = vl[4 * q]; lab.y = vl[4 * q + 1]; lab.z = vl[4 * q + 2]; lab.w = vl[4 * q + 3];
+            } else {
+                lab = reinterpret_cast<const uint4 *>(labels)[q];
+            }
+            uint32_t r[4] = {lab.x, lab.y, lab.z, lab.w};
+            uint32_t flip = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                uint32_t c = r[k], d;
+                if (kWriteLabels) {
+                    while ((d = vl[c]) != c) c = d;
+                } else {
+                    while ((d = labels[c]) != c) c = d;
+                }
+                r[k] = c;
+                flip |= (c & 1u) << (8 * k);
+            }
+            uint32_t *sw = reinterpret_cast<uint32_t *>(spins) + q;
+            *sw ^= flip;
+            if (kWriteLabels) {
+                labels[4 * q] = r[0]; labels[4 * q + 1] = r[1]; labels[4 * q + 2] = r[2]; labels[4 * q + 3] = r[3];
+            }
+        }
+    } else {
+        for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+            uint32_t c = vl[i], d;
+            while ((d = vl[c]) != c) c = d;
+            spins[i] ^= (uint8_t)(c & 1u);
+            if (kWriteLabels)
+                labels[i] = c;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_measure(const uint32_t L0, const uint32_t L1, const uint8_t *__restrict__ spins,
+                                                 Obs *obs, long long *series, const unsigned long long cap,
+                                                 const int accumulate)
+{
+    long long e = 0, m = 0;
+    const size_t n = (size_t)L0 * L1;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint32_t y = (uint32_t)(i / L0), x = (uint32_t)(i - (size_t)y * L0);
+        const int s = 2 * spins[i] - 1;
+        const int r = 2 * spins[(size_t)y * L0 + (x + 1 == L0 ? 0 : x + 1)] - 1;
+        const int d = 2 * spins[(size_t)(y + 1 == L1 ? 0 : y + 1) * L0 + x] - 1;
+        e += s * (r + d);
+        m += s;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        e += __shfl_xor_sync(0xffffffffu, e, o);
+        m += __shfl_xor_sync(0xffffffffu, m, o);
+    }
+    __shared__ long long se[8], sm[8];
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        se[w] = e;
+        sm[w] = m;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long be = 0, bm = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+            be += se[k];
+            bm += sm[k];
+        }
+        atomicAdd(&obs->e, (unsigned long long)be);
+        atomicAdd(&obs->m, (unsigned long long)bm);
+        __threadfence();
+        const unsigned int ticket = atomicAdd(&obs->done, 1u);
+        if (ticket == gridDim.x - 1) {
+            __threadfence();
+            const long long te = (long long)atomicAdd(&obs->e, 0ull);
+            const long long tm = (long long)atomicAdd(&obs->m, 0ull);
+            obs->last_e = te;
+            obs->last_m = tm;
+            if (accumulate) {
+                const double E = -(double)te / (double)n, M = (double)tm / (double)n;
+                obs->acc[0] += E;
+                obs->acc[1] += E * E;
+                obs->acc[2] += fabs(M);
+                obs->acc[3] += 1.0;
+                const unsigned long long k = obs->n_samples;
+                if (k < cap) {
+                    series[2 * k] = te;
+                    series[2 * k + 1] = tm;
+                }
+                obs->n_samples = k + 1;
+            }
+            obs->e = 0;
+            obs->m = 0;
+            obs->done = 0;
+        }
+    }
+}
+
+// LCG32_State<W>::Init for every tile (random/src/lcg32.cpp:138-160), seeds seed_base + tile.
+template <int W>
+__global__ void k_rng_init(const uint32_t n_tiles, const uint32_t seed_base, uint32_t *state, uint8_t *sel,
+                           uint32_t *iter)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_tiles)
+        return;
+    uint64_t x = drand48_seed(seed_base + t);
+    uint32_t s[W];
+#pragma unroll
+    for (int i = 0; i < W; ++i) {
+        x = drand48_step(x);
+        s[i] = ((uint32_t)__dmul_rn(1000.0, drand48_value(x))) % 5u;
+        sel[(size_t)t * W + i] = (uint8_t)s[i];
+    }
+    x = drand48_step(x);
+    uint32_t v = lcg_param_a(s[0]) * ((uint32_t)__dmul_rn(4026531839.0, drand48_value(x)) + 1u) + lcg_param_c(s[0]);
+    state[(size_t)t * W] = v;
+#pragma unroll
+    for (int i = 1; i < W; ++i) {
+        v = lcg_param_a(s[i]) * v + lcg_param_c(s[i]);
+        state[(size_t)t * W + i] = v;
+    }
+    iter[t] = 0;
+}
+
+// Hot start of Lattice<2> (ising/src/lattice.cpp:122-124): site i takes drand48 draw i + 1
+// after srand48(seed); drand48() < 0.5 iff bit 47 of the 48-bit state is clear.
+__global__ void k_hot_start(const size_t n, const uint32_t seed, uint8_t *spins)
+{
+    constexpr uint32_t kChunk = 64;
+    const size_t first = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) * kChunk;
+    if (first >= n)
+        return;
+    uint64_t A, C;
+    drand48_jump(first, A, C);
+    uint64_t x = (A * drand48_seed(seed) + C) & kDrandMask;
+    const size_t last = first + kChunk < n ? first + kChunk : n;
+    for (size_t i = first; i < last; ++i) {
+        x = drand48_step(x);
+        spins[i] = (uint8_t)(x >> 47);
+    }
+}
+
+__global__ void k_fill(const size_t n, const uint8_t v, uint8_t *p)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        p[i] = v;
+}
+
+__global__ void k_check_spins(const size_t n, const uint8_t *p, unsigned int *bad)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        if (p[i] > 1)
+            atomicOr(bad, 1u);
+}
+
+}  // namespace swb
+
+// ------------------------------------------------------------------------------------------
+// the handle
+
+using namespace swb;
+
+struct swb_lattice {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    Geo g{};
+    uint32_t W = 16, seed_base = 1, n_tiles = 0, n_blocks = 0, smem_assign = 0;
+    size_t n = 0;
+    uint8_t *spins = nullptr;
+    uint32_t *labels = nullptr;
+    uint32_t *rng_state = nullptr;
+    uint8_t *rng_sel = nullptr;
+    uint32_t *rng_iter = nullptr;
+    uint32_t *edge = nullptr;
+    Obs *obs = nullptr;
+    long long *series = nullptr;
+    unsigned long long series_cap = 0;
+    unsigned int *scratch_flag = nullptr;
+    int flip_grid = 0, measure_grid = 0;
+};
+
+namespace {
+
+const uint32_t kFlipThreads = 256;
+
+int set_device(const swb_lattice *h)
+{
+    SWB_CUDA(cudaSetDevice(h->device));
+    return SWB_OK;
+}
+
+template <int W>
+int launch_assign_w(swb_lattice *h, float p_add, uint8_t *dbg_bonds, uint32_t *dbg_assign)
+{
+    const Geo &g = h->g;
+    const dim3 grid(g.nbx, g.nby), block(g.TBX * g.TBY * W);
+    k_assign<W><<<grid, block, h->smem_assign, h->stream>>>(g, h->spins, h->labels, h->rng_state, h->rng_sel,
+                                                            h->rng_iter, p_add, h->edge, dbg_bonds, dbg_assign);
+    SWB_LAUNCHED();
+    return SWB_OK;
+}
+
+int launch_assign(swb_lattice *h, float p_add, uint8_t *dbg_bonds, uint32_t *dbg_assign)
+{
+    switch (h->W) {
+    case 8: return launch_assign_w<8>(h, p_add, dbg_bonds, dbg_assign);
+    case 16: return launch_assign_w<16>(h, p_add, dbg_bonds, dbg_assign);
+    case 32: return launch_assign_w<32>(h, p_add, dbg_bonds, dbg_assign);
+    }
+    return fail(SWB_ERR_ARGUMENT, "unsupported lcg width %u", h->W);
+}
+
+int launch_sweep(swb_lattice *h, float p_add, bool write_labels, uint8_t *dbg_bonds, uint32_t *dbg_assign)
+{
+    int rc = launch_assign(h, p_add, dbg_bonds, dbg_assign);
+    if (rc)
+        return rc;
+    k_merge<<<h->n_blocks, h->g.BX + h->g.BY, 0, h->stream>>>(h->g, h->edge, h->labels);
+    SWB_LAUNCHED();
+    if (write_labels)
+        k_flip<true><<<h->flip_grid, kFlipThreads, 0, h->stream>>>((uint32_t)h->n, h->spins, h->labels);
+    else
+        k_flip<false><<<h->flip_grid, kFlipThreads, 0, h->stream>>>((uint32_t)h->n, h->spins, h->labels);
+    SWB_LAUNCHED();
+    return SWB_OK;
+}
+
+int launch_measure(swb_lattice *h, int accumulate)
+{
+    k_measure<<<h->measure_grid, 256, 0, h->stream>>>(h->g.L0, h->g.L1, h->spins, h->obs, h->series, h->series_cap,
+                                                       accumulate);
+    SWB_LAUNCHED();
+    return SWB_OK;
+}
+
+bool valid_width(uint32_t W) { return W == 8 || W == 16 || W == 32; }
+
+int index_of_pair(uint32_t a, uint32_t c)
+{
+    for (uint32_t s = 0; s < 5; ++s)
+        if (lcg_param_a(s) == a && lcg_param_c(s) == c)
+            return (int)s;
+    return -1;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *swb_version(void) { return "swb200 0.1 (sm_100a)"; }
+
+int swb_device_count(int *count)
+{
+    if (!count)
+        return fail(SWB_ERR_ARGUMENT, "count is NULL");
+    *count = 0;
+    const cudaError_t e = cudaGetDeviceCount(count);
+    if (e != cudaSuccess) {
+        *count = 0;
+        cudaGetLastError();
+    }
+    return SWB_OK;
+}
+
+const char *swb_last_error(void) { return g_last_error.c_str(); }
+
+uint64_t swb_kernel_launches(void) { return g_launches.load(); }
+
+float swb_p_add(float temperature) { return 1.0f - static_cast<float>(std::exp(-2.0f / temperature)); }
+
+int swb_create(swb_lattice **out, uint32_t L0, uint32_t L1, uint32_t tile_x, uint32_t tile_y, uint32_t lcg_width,
+               uint32_t seed_base, int device)
+{
+    if (!out)
+        return fail(SWB_ERR_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    if (L0 == 0 || L1 == 0 || (L0 % 2) || (L1 % 2))
+        return fail(SWB_ERR_ARGUMENT, "SwendsenWang_2D implementation requires evenly sized lattice (%u x %u)", L0, L1);
+    if ((uint64_t)L0 * L1 > 0xFFFFFFFFull)
+        return fail(SWB_ERR_ARGUMENT, "lattice of %u x %u sites exceeds 32-bit labels", L0, L1);
+    if (!(tile_x == 8 || tile_x == 16 || tile_x == 32) || tile_y < 2 || tile_y > 32)
+        return fail(SWB_ERR_ARGUMENT, "unsupported tile %u x %u (tile_x in {8,16,32}, 2 <= tile_y <= 32)", tile_x, tile_y);
+    if (!valid_width(lcg_width))
+        return fail(SWB_ERR_ARGUMENT, "unsupported lcg32 width %u (8, 16 or 32)", lcg_width);
+    swb_lattice *h = new swb_lattice();
+    h->device = device;
+    h->W = lcg_width;
+    h->seed_base = seed_base;
+    h->g = make_geo(L0, L1, tile_x, tile_y, lcg_width);
+    h->n = (size_t)L0 * L1;
+    h->n_tiles = h->g.n0 * h->g.n1;
+    h->n_blocks = h->g.nbx * h->g.nby;
+    h->smem_assign = assign_smem(h->g).total;
+    auto cleanup = [&](int rc) {
+        swb_destroy(h);
+        return rc;
+    };
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess)
+        return cleanup(fail(SWB_ERR_CUDA, "cudaSetDevice(%d): %s", device, cudaGetErrorString(e)));
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+#define SWB_TRY(call)                                                                                \
+    do {                                                                                             \
+        cudaError_t err__ = (call);                                                                  \
+        if (err__ != cudaSuccess)                                                                    \
+            return cleanup(fail(SWB_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(err__)));   \
+    } while (0)
+    SWB_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    SWB_TRY(cudaMalloc(&h->spins, h->n + 16));
+    SWB_TRY(cudaMalloc(&h->labels, h->n * sizeof(uint32_t) + 16));
+    SWB_TRY(cudaMalloc(&h->rng_state, (size_t)h->n_tiles * h->W * sizeof(uint32_t)));
+    SWB_TRY(cudaMalloc(&h->rng_sel, (size_t)h->n_tiles * h->W));
+    SWB_TRY(cudaMalloc(&h->rng_iter, (size_t)h->n_tiles * sizeof(uint32_t)));
+    SWB_TRY(cudaMalloc(&h->edge, (size_t)h->n_blocks * kEdgeWords * sizeof(uint32_t)));
+    SWB_TRY(cudaMalloc(&h->obs, sizeof(Obs)));
+    h->series_cap = 1ull << 20;
+    SWB_TRY(cudaMalloc(&h->series, h->series_cap * 2 * sizeof(long long)));
+    SWB_TRY(cudaMalloc(&h->scratch_flag, sizeof(unsigned int)));
+    SWB_TRY(cudaMemsetAsync(h->spins, 0, h->n + 16, h->stream));
+    SWB_TRY(cudaMemsetAsync(h->obs, 0, sizeof(Obs), h->stream));
+    const size_t nq = (h->n % 4 == 0) ? h->n / 4 : h->n;
+    h->flip_grid = (int)std::min<size_t>((nq + kFlipThreads - 1) / kFlipThreads, (size_t)sms * 16);
+    h->measure_grid = (int)std::min<size_t>((h->n + 255) / 256, (size_t)sms * 8);
+    if (h->flip_grid < 1) h->flip_grid = 1;
+    if (h->measure_grid < 1) h->measure_grid = 1;
+    switch (h->W) {
+    case 8: k_rng_init<8><<<(h->n_tiles + 127) / 128, 128, 0, h->stream>>>(h->n_tiles, seed_base, h->rng_state, h->rng_sel, h->rng_iter); break;
+    case 16: k_rng_init<16><<<(h->n_tiles + 127) / 128, 128, 0, h->stream>>>(h->n_tiles, seed_base, h->rng_state, h->rng_sel, h->rng_iter); break;
+    default: k_rng_init<32><<<(h->n_tiles + 127) / 128, 128, 0, h->stream>>>(h->n_tiles, seed_base, h->rng_state, h->rng_sel, h->rng_iter); break;
+    }
+    g_launches.fetch_add(1);
+    SWB_TRY(cudaGetLastError());
+    SWB_TRY(cudaStreamSynchronize(h->stream));
+#undef SWB_TRY
+    *out = h;
+    return SWB_OK;
+}
+
+int swb_destroy(swb_lattice *h)
+{
+    if (!h)
+        return SWB_OK;
+    cudaSetDevice(h->device);
+    if (h->stream)
+        cudaStreamSynchronize(h->stream);
+    cudaFree(h->spins);
+    cudaFree(h->labels);
+    cudaFree(h->rng_state);
+    cudaFree(h->rng_sel);
+    cudaFree(h->rng_iter);
+    cudaFree(h->edge);
+    cudaFree(h->obs);
+    cudaFree(h->series);
+    cudaFree(h->scratch_flag);
+    if (h->stream)
+        cudaStreamDestroy(h->stream);
+    delete h;
+    return SWB_OK;
+}
+
+int swb_set_spins(swb_lattice *h, const uint8_t *host_spins)
+{
+    if (!h || !host_spins)
+        return fail(SWB_ERR_ARGUMENT, "NULL argument");
+    if (int rc = set_device(h))
+        return rc;
+    SWB_CUDA(cudaMemcpyAsync(h->spins, host_spins, h->n, cudaMemcpyHostToDevice, h->stream));
+    SWB_CUDA(cudaMemsetAsync(h->scratch_flag, 0, sizeof(unsigned int), h->stream));
+    k_check_spins<<<h->measure_grid, 256, 0, h->stream>>>(h->n, h->spins, h->scratch_flag);
+    SWB_LAUNCHED();
+    unsigned int bad = 0;
+    SWB_CUDA(cudaMemcpyAsync(&bad, h->scratch_flag, sizeof(bad), cudaMemcpyDeviceToHost, h->stream));
+    SWB_CUDA(cudaStreamSynchronize(h->stream));
+    if (bad)
+        return fail(SWB_ERR_ARGUMENT, "spins must be 0 or 1");
+    return SWB_OK;
+}
+
+int swb_get_spins(swb_lattice *h, uint8_t *host_spins)
+{
+    if (!h || !host_spins)
+        return fail(SWB_ERR_ARGUMENT, "NULL argument");
+    if (int rc = set_device(h))
+        return rc;
+    SWB_CUDA(cudaMemcpyAsync(host_spins, h->spins, h->n, cudaMemcpyDeviceToHost, h->stream));
+    SWB_CUDA(cudaStreamSynchronize(h->stream));
+    return SWB_OK;
+}
+
+int swb_hot_start(swb_lattice *h, uint32_t seed)
+{
+    if (!h)
+        return fail(SWB_ERR_ARGUMENT, "NULL handle");
+    if (int rc = set_device(h))
+        return rc;
+    const size_t chunks = (h->n + 63) / 64;
+    k_hot_start<<<(unsigned)((chunks + 255) / 256), 256, 0, h->stream>>>(h->n, seed, h->spins);
+    SWB_LAUNCHED();
+    return SWB_OK;
+}
+
+int swb_cold_start(swb_lattice *h, uint8_t value)
+{
+    if (!h || value > 1)
+        return fail(SWB_ERR_ARGUMENT, "cold start value must be 0 or 1");
+    if (int rc = set_device(h))
+        return rc;
+    k_fill<<<h->measure_grid, 256, 0, h->stream>>>(h->n, value, h->spins);
+    SWB_LAUNCHED();
+    return SWB_OK;
+}
+
+int swb_sweep(swb_lattice *h, float temperature, uint32_t n_sweeps, uint32_t measure_every)
+{
+    if (!h)
+        return fail(SWB_ERR_ARGUMENT, "NULL handle");
+    if (!(temperature > 0.0f) || !std::isfinite(temperature))
+        return fail(SWB_ERR_ARGUMENT, "temperature must be positive and finite");
+    if (int rc = set_device(h))
+        return rc;
+    const float p_add = swb_p_add(temperature);
+    for (uint32_t s = 1; s <= n_sweeps; ++s) {
+        if (int rc = launch_sweep(h, p_add, false, nullptr, nullptr))
+            return rc;
+        if (measure_every && (s % measure_every) == 0)
+            if (int rc = launch_measure(h, 1))
+                return rc;
+    }
+    return SWB_OK;
+}
+
+int swb_sweep_recorded(swb_lattice *h, float temperature, uint8_t *bonds, uint32_t *labels_assign,
+                       uint32_t *labels_final)
+{
+    if (!h)
+        return fail(SWB_ERR_ARGUMENT, "NULL handle");
+    if (!(temperature > 0.0f) || !std::isfinite(temperature))
+        return fail(SWB_ERR_ARGUMENT, "temperature must be positive and finite");
+    if (int rc = set_device(h))
+        return rc;
+    uint8_t *d_bonds = nullptr;
+    uint32_t *d_assign = nullptr;
+    SWB_CUDA(cudaMallocAsync(&d_bonds, h->n, h->stream));
+    SWB_CUDA(cudaMallocAsync(&d_assign, h->n * sizeof(uint32_t), h->stream));
+    int rc = launch_sweep(h, swb_p_add(temperature), true, d_bonds, d_assign);
+    if (rc == SWB_OK) {
+        if (bonds)
+            SWB_CUDA(cudaMemcpyAsync(bonds, d_bonds, h->n, cudaMemcpyDeviceToHost, h->stream));
+        if (labels_assign)
+            SWB_CUDA(cudaMemcpyAsync(labels_assign, d_assign, h->n * 4, cudaMemcpyDeviceToHost, h->stream));
+        if (labels_final)
+            SWB_CUDA(cudaMemcpyAsync(labels_final, h->labels, h->n * 4, cudaMemcpyDeviceToHost, h->stream));
+    }
+    cudaFreeAsync(d_bonds, h->stream);
+    cudaFreeAsync(d_assign, h->stream);
+    SWB_CUDA(cudaStreamSynchronize(h->stream));
+    return rc;
+}
+
+int swb_synchronize(swb_lattice *h)
+{
+    if (!h)
+        return fail(SWB_ERR_ARGUMENT, "NULL handle");
+    if (int rc = set_device(h))
+        return rc;
+    SWB_CUDA(cudaStreamSynchronize(h->stream));
+    return SWB_OK;
+}
+
+int swb_energy_magnetization(swb_lattice *h, double *out, int64_t *e_sum, int64_t *m_sum)
+{
+    if (!h)
+        return fail(SWB_ERR_ARGUMENT, "NULL handle");
+    if (int rc = set_device(h))
+        return rc;
+    if (int rc = launch_measure(h, 0))
+        return rc;
+    Obs o;
+    SWB_CUDA(cudaMemcpyAsync(&o, h->obs, sizeof(Obs), cudaMemcpyDeviceToHost, h->stream));
+    SWB_CUDA(cudaStreamSynchronize(h->stream));
+    if (out) {
+        out[0] = -(double)o.last_e / (double)h->n;
+        out[1] = (double)o.last_m / (double)h->n;
+    }
+    if (e_sum) *e_sum = o.last_e;
+    if (m_sum) *m_sum = o.last_m;
+    return SWB_OK;
+}
+
+int swb_accumulators(swb_lattice *h, double *out)
+{
+    if (!h || !out)
+        return fail(SWB_ERR_ARGUMENT, "NULL argument");
+    if (int rc = set_device(h))
+        return rc;
+    Obs o;
+    SWB_CUDA(cudaMemcpyAsync(&o, h->obs, sizeof(Obs), cudaMemcpyDeviceToHost, h->stream));
+    SWB_CUDA(cudaStreamSynchronize(h->stream));
+    std::memcpy(out, o.acc, sizeof(o.acc));
+    return SWB_OK;
+}
+
+int swb_reset_accumulators(swb_lattice *h)
+{
+    if (!h)
+        return fail(SWB_ERR_ARGUMENT, "NULL handle");
+    if (int rc = set_device(h))
+        return rc;
+    SWB_CUDA(cudaMemsetAsync(h->obs, 0, sizeof(Obs), h->stream));
+    return SWB_OK;
+}
+
+int swb_samples(swb_lattice *h, int64_t *em, uint64_t capacity, uint64_t *count)
+{
+    if (!h || !count)
+        return fail(SWB_ERR_ARGUMENT, "NULL argument");
+    if (int rc = set_device(h))
+        return rc;
+    Obs o;
+    SWB_CUDA(cudaMemcpyAsync(&o, h->obs, sizeof(Obs), cudaMemcpyDeviceToHost, h->stream));
+    SWB_CUDA(cudaStreamSynchronize(h->stream));
+    *count = o.n_samples;
+    if (o.n_samples > h->series_cap)
+        return fail(SWB_ERR_CAPACITY, "%llu samples recorded, series keeps %llu", o.n_samples, h->series_cap);
+    const uint64_t k = o.n_samples < capacity ? o.n_samples : capacity;
+    if (k && em) {
+        SWB_CUDA(cudaMemcpyAsync(em, h->series, k * 2 * sizeof(long long), cudaMemcpyDeviceToHost, h->stream));
+        SWB_CUDA(cudaStreamSynchronize(h->stream));
+    }
+    return SWB_OK;
+}
+
+int swb_rng_shape(swb_lattice *h, uint32_t *n_tiles, uint32_t *lcg_width)
+{
+    if (!h)
+        return fail(SWB_ERR_ARGUMENT, "NULL handle");
+    if (n_tiles) *n_tiles = h->n_tiles;
+    if (lcg_width) *lcg_width = h->W;
+    return SWB_OK;
+}
+
+int swb_get_rng(swb_lattice *h, uint32_t *state, uint32_t *a, uint32_t *c, uint32_t *iteration)
+{
+    if (!h || !state || !a || !c || !iteration)
+        return fail(SWB_ERR_ARGUMENT, "NULL argument");
+    if (int rc = set_device(h))
+        return rc;
+    const size_t nw = (size_t)h->n_tiles * h->W;
+    std::vector<uint8_t> sel(nw);
+    SWB_CUDA(cudaMemcpyAsync(state, h->rng_state, nw * 4, cudaMemcpyDeviceToHost, h->stream));
+    SWB_CUDA(cudaMemcpyAsync(sel.data(), h->rng_sel, nw, cudaMemcpyDeviceToHost, h->stream));
+    SWB_CUDA(cudaMemcpyAsync(iteration, h->rng_iter, (size_t)h->n_tiles * 4, cudaMemcpyDeviceToHost, h->stream));
+    SWB_CUDA(cudaStreamSynchronize(h->stream));
+    for (size_t i = 0; i < nw; ++i) {
+        a[i] = lcg_param_a(sel[i]);
+        c[i] = lcg_param_c(sel[i]);
+    }
+    return SWB_OK;
+}
+
+int swb_set_rng(swb_lattice *h, const uint32_t *state, const uint32_t *a, const uint32_t *c,
+                const uint32_t *iteration)
+{
+    if (!h || !state || !a || !c || !iteration)
+        return fail(SWB_ERR_ARGUMENT, "NULL argument");
+    if (int rc = set_device(h))
+        return rc;
+    const size_t nw = (size_t)h->n_tiles * h->W;
+    std::vector<uint8_t> sel(nw);
+    for (size_t i = 0; i < nw; ++i) {
+        const int s = index_of_pair(a[i], c[i]);
+        if (s < 0)
+            return fail(SWB_ERR_ARGUMENT, "lane %zu: (a, c) = (%u, %u) is not an lcg32 parameter pair", i, a[i], c[i]);
+        sel[i] = (uint8_t)s;
+    }
+    SWB_CUDA(cudaMemcpyAsync(h->rng_state, state, nw * 4, cudaMemcpyHostToDevice, h->stream));
+    SWB_CUDA(cudaMemcpyAsync(h->rng_sel, sel.data(), nw, cudaMemcpyHostToDevice, h->stream));
+    SWB_CUDA(cudaMemcpyAsync(h->rng_iter, iteration, (size_t)h->n_tiles * 4, cudaMemcpyHostToDevice, h->stream));
+    SWB_CUDA(cudaStreamSynchronize(h->stream));
+    return SWB_OK;
+}
+
+int swb_device_buffers(swb_lattice *h, void **spins, void **labels)
+{
+    if (!h)
+        return fail(SWB_ERR_ARGUMENT, "NULL handle");
+    if (spins) *spins = h->spins;
+    if (labels) *labels = h->labels;
+    return SWB_OK;
+}
+
+int swb_launches_per_sweep(swb_lattice *h, uint32_t *launches)
+{
+    if (!h || !launches)
+        return fail(SWB_ERR_ARGUMENT, "NULL argument");
+    *launches = 3;
+    return SWB_OK;
+}
+
+int swb_sweep_timed(swb_lattice *h, float temperature, uint32_t n_sweeps, int per_kernel, float *ms)
+{
+    if (!h || !ms)
+        return fail(SWB_ERR_ARGUMENT, "NULL argument");
+    if (!(temperature > 0.0f) || !std::isfinite(temperature))
+        return fail(SWB_ERR_ARGUMENT, "temperature must be positive and finite");
+    if (int rc = set_device(h))
+        return rc;
+    const float p_add = swb_p_add(temperature);
+    ms[0] = ms[1] = ms[2] = ms[3] = 0.0f;
+    cudaEvent_t ev[5];
+    for (auto &e : ev)
+        SWB_CUDA(cudaEventCreate(&e));
+    int rc = SWB_OK;
+    SWB_CUDA(cudaEventRecord(ev[0], h->stream));
+    for (uint32_t s = 0; s < n_sweeps && rc == SWB_OK; ++s) {
+        if (!per_kernel) {
+            rc = launch_sweep(h, p_add, false, nullptr, nullptr);
+            continue;
+        }
+        SWB_CUDA(cudaEventRecord(ev[1], h->stream));
+        if ((rc = launch_assign(h, p_add, nullptr, nullptr)))
+            break;
+        SWB_CUDA(cudaEventRecord(ev[2], h->stream));
+        k_merge<<<h->n_blocks, h->g.BX + h->g.BY, 0, h->stream>>>(h->g, h->edge, h->labels);
+        SWB_LAUNCHED();
+        SWB_CUDA(cudaEventRecord(ev[3], h->stream));
+        k_flip<false><<<h->flip_grid, kFlipThreads, 0, h->stream>>>((uint32_t)h->n, h->spins, h->labels);
+        SWB_LAUNCHED();
+        SWB_CUDA(cudaEventRecord(ev[4], h->stream));
+        SWB_CUDA(cudaEventSynchronize(ev[4]));
+        float t;
+        SWB_CUDA(cudaEventElapsedTime(&t, ev[1], ev[2]));
+        ms[1] += t;
+        SWB_CUDA(cudaEventElapsedTime(&t, ev[2], ev[3]));
+        ms[2] += t;
+        SWB_CUDA(cudaEventElapsedTime(&t, ev[3], ev[4]));
+        ms[3] += t;
+    }
+    SWB_CUDA(cudaEventRecord(ev[4], h->stream));
+    SWB_CUDA(cudaEventSynchronize(ev[4]));
+    SWB_CUDA(cudaEventElapsedTime(&ms[0], ev[0], ev[4]));
+    for (auto &e : ev)
+        cudaEventDestroy(e);
+    return rc;
+}
+
+int swb_host_alloc(void **ptr, size_t bytes)
+{
+    if (!ptr)
+        return fail(SWB_ERR_ARGUMENT, "ptr is NULL");
+    SWB_CUDA(cudaHostAlloc(ptr, bytes ? bytes : 1, cudaHostAllocDefault));
+    return SWB_OK;
+}
+
+int swb_host_free(void *ptr)
+{
+    if (ptr)
+        SWB_CUDA(cudaFreeHost(ptr));
+    return SWB_OK;
+}
+
+int swb_update_host(swb_lattice *h, float temperature, const uint8_t *spins_in, uint8_t *spins_out, double *em_out)
+{
+    if (!h || !spins_in || !spins_out)
+        return fail(SWB_ERR_ARGUMENT, "NULL argument");
+    if (!(temperature > 0.0f) || !std::isfinite(temperature))
+        return fail(SWB_ERR_ARGUMENT, "temperature must be positive and finite");
+    if (int rc = set_device(h))
+        return rc;
+    SWB_CUDA(cudaMemcpyAsync(h->spins, spins_in, h->n, cudaMemcpyHostToDevice, h->stream));
+    if (int rc = launch_sweep(h, swb_p_add(temperature), false, nullptr, nullptr))
+        return rc;
+    SWB_CUDA(cudaMemcpyAsync(spins_out, h->spins, h->n, cudaMemcpyDeviceToHost, h->stream));
+    if (em_out) {
+        if (int rc = launch_measure(h, 0))
+            return rc;
+        Obs o;
+        SWB_CUDA(cudaMemcpyAsync(&o, h->obs, sizeof(Obs), cudaMemcpyDeviceToHost, h->stream));
+        SWB_CUDA(cudaStreamSynchronize(h->stream));
+        em_out[0] = -(double)o.last_e / (double)h->n;
+        em_out[1] = (double)o.last_m / (double)h->n;
+    }
+    SWB_CUDA(cudaStreamSynchronize(h->stream));
+    return SWB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,206 @@
+/*
+ * swb200.h -- C ABI of the B200-native Swendsen-Wang engine for the 2D Ising model.
+ *
+ * This is the boundary a host program (C, C++, Python ctypes, ...) binds.  It carries
+ * only plain pointers and sizes.  Every function returns SWB_OK (0) or a non-zero
+ * status; swb_last_error() gives the message of the last failure on the calling thread.
+ * Host buffers belong to the caller; device buffers belong to the engine handle.  A
+ * handle is driven by one host thread at a time (it owns one CUDA stream).
+ *
+ * Conventions (identical to the reference flwende/computational_physics):
+ *   spins   uint8 0/1, row-major, x fastest            (ising/include/lattice.hpp:24)
+ *   labels  uint32, minimum global site index of the cluster
+ *   bonds   uint8 per site: bit 0 = +x bond, bit 1 = +y bond (periodic)
+ *   lcg32   one stream per tile, tiles row-major, seeded seed_base + tile id; the stream
+ *           state is exchanged in the reference's LCG32_State<W> terms: W state words,
+ *           W multipliers a, W increments c, one iteration counter per tile
+ *           (random/include/random/lcg32.hpp:27-58)
+ */
+#ifndef SWB200_H
+#define SWB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SWB_OK 0
+#define SWB_ERR_ARGUMENT 1   /* invalid size, extent, tile, width or pointer            */
+#define SWB_ERR_CUDA 2       /* a CUDA runtime call failed                              */
+#define SWB_ERR_STATE 3      /* call not valid in the handle's current state            */
+#define SWB_ERR_CAPACITY 4   /* request exceeds a configured capacity (samples, budget) */
+
+typedef struct swb_lattice swb_lattice;
+
+/* Library version string. */
+const char *swb_version(void);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *swb_last_error(void);
+
+/* Number of visible CUDA devices (0 when there is no GPU or driver). */
+int swb_device_count(int *count);
+
+/* Number of kernel launches this process has issued through the library (all handles). */
+uint64_t swb_kernel_launches(void);
+
+/* ---- single lattice: the drop-in for SwendsenWang_2D<LCG32, Target>::Update ------------- */
+
+/* Creates an L0 x L1 periodic lattice on CUDA device `device` with tiles tile_x x tile_y
+ * and lcg32 streams of `lcg_width` lanes seeded seed_base + tile id.  Replaces
+ * SwendsenWang_2D::Initialize (ising/src/swendsen_wang.cpp:148-199): extents must be
+ * even (:154-155); labels fit uint32 (swendsen_wang.hpp:29-30).  tile_x in {8, 16, 32},
+ * 2 <= tile_y <= 32, lcg_width in {8, 16, 32}.  Spins start all 0. */
+int swb_create(swb_lattice **out, uint32_t L0, uint32_t L1, uint32_t tile_x, uint32_t tile_y,
+               uint32_t lcg_width, uint32_t seed_base, int device);
+
+/* Releases every device buffer of the handle (reference: GpuPointer deleters,
+ * utility/hip/hip.hpp:18-39). */
+int swb_destroy(swb_lattice *h);
+
+/* Copies host spins (L0*L1 bytes, 0/1) to the device: Lattice<2>::InitializeGpuSpins
+ * (ising/src/lattice.cpp:179-194).  Values other than 0/1 are rejected. */
+int swb_set_spins(swb_lattice *h, const uint8_t *host_spins);
+
+/* Copies the device spins to the host (L0*L1 bytes). */
+int swb_get_spins(swb_lattice *h, uint8_t *host_spins);
+
+/* Hot start on the device, bit-identical to Lattice<2>'s constructor with srand48(seed)
+ * (ising/src/lattice.cpp:113-125; the reference always uses seed 1). */
+int swb_hot_start(swb_lattice *h, uint32_t seed);
+
+/* All spins set to `value` (0 or 1): a cold start. */
+int swb_cold_start(swb_lattice *h, uint8_t value);
+
+/* p_add = 1 - exp(-2/T) in float, as ising/src/swendsen_wang.cpp:207. */
+float swb_p_add(float temperature);
+
+/* n_sweeps sweeps at `temperature`: SwendsenWang_2D::Update (ising/src/swendsen_wang.cpp:201-219)
+ * -- bond activation + tile labelling, boundary merge, label resolution, cluster flip.  If
+ * measure_every > 0, after every measure_every-th sweep the energy and magnetisation are
+ * accumulated on the device (E, E^2, |M| in FP64, and the exact integer sums per sample).
+ * Asynchronous on the handle's stream; errors of the launches are reported. */
+int swb_sweep(swb_lattice *h, float temperature, uint32_t n_sweeps, uint32_t measure_every);
+
+/* Like swb_sweep with n_sweeps = 1, additionally dumping this sweep's stages to HOST buffers
+ * (each may be NULL): bonds (uint8 per site), labels after tile-local labelling
+ * (AssignLabels), labels after resolution (ResolveLabels).  Synchronous. */
+int swb_sweep_recorded(swb_lattice *h, float temperature, uint8_t *bonds, uint32_t *labels_assign,
+                       uint32_t *labels_final);
+
+/* Waits for all work of the handle. */
+int swb_synchronize(swb_lattice *h);
+
+/* Energy and magnetisation per site of the current spins (Lattice<2>::GetEnergyAndMagnetization,
+ * ising/src/lattice.cpp:127-177), reduced on the device: out[0] = E/N, out[1] = M/N.
+ * The exact integer sums go to e_sum / m_sum when non-NULL. */
+int swb_energy_magnetization(swb_lattice *h, double *out, int64_t *e_sum, int64_t *m_sum);
+
+/* Observable accumulators since the last reset: out[0] = sum E/N, out[1] = sum (E/N)^2,
+ * out[2] = sum |M/N|, out[3] = number of samples.  Synchronous. */
+int swb_accumulators(swb_lattice *h, double *out);
+
+/* Clears the accumulators and the sample series. */
+int swb_reset_accumulators(swb_lattice *h);
+
+/* Copies up to `capacity` recorded samples (exact integer sums e, m per measured sweep,
+ * interleaved e0, m0, e1, m1, ...) to the host; *count receives the number recorded. */
+int swb_samples(swb_lattice *h, int64_t *em, uint64_t capacity, uint64_t *count);
+
+/* Number of tiles and the lane count of the handle's lcg32 streams. */
+int swb_rng_shape(swb_lattice *h, uint32_t *n_tiles, uint32_t *lcg_width);
+
+/* Exports / imports the per-tile lcg32 streams in LCG32_State<W> terms (arrays n_tiles*W,
+ * n_tiles).  Import rejects (a, c) pairs that are not one of the reference's five
+ * parameter pairs (random/src/lcg32.cpp:128-135). */
+int swb_get_rng(swb_lattice *h, uint32_t *state, uint32_t *a, uint32_t *c, uint32_t *iteration);
+int swb_set_rng(swb_lattice *h, const uint32_t *state, const uint32_t *a, const uint32_t *c,
+                const uint32_t *iteration);
+
+/* Device pointers of the spin and label arrays (for zero-copy interop; valid until destroy). */
+int swb_device_buffers(swb_lattice *h, void **spins, void **labels);
+
+/* Number of kernel launches one plain sweep issues on this handle. */
+int swb_launches_per_sweep(swb_lattice *h, uint32_t *launches);
+
+/* n_sweeps sweeps like swb_sweep (no measurement), timed with CUDA events on the handle's
+ * stream.  ms[0] = total elapsed; when per_kernel != 0 an event pair brackets every launch
+ * and ms[1..3] = summed durations of the assign, merge and flip kernels.  Synchronous. */
+int swb_sweep_timed(swb_lattice *h, float temperature, uint32_t n_sweeps, int per_kernel, float *ms);
+
+/* Page-locked host memory for fast host<->device copies (cudaHostAlloc / cudaFreeHost). */
+int swb_host_alloc(void **ptr, size_t bytes);
+int swb_host_free(void *ptr);
+
+/* One sweep through HOST spin buffers, as the reference's Lattice<2> keeps them: copy
+ * spins_in to the device, sweep, read the spins back to spins_out and the energy and
+ * magnetisation per site to em_out[2] (may be NULL).  Synchronous. */
+int swb_update_host(swb_lattice *h, float temperature, const uint8_t *spins_in, uint8_t *spins_out,
+                    double *em_out);
+
+/* ---- batched lattices: many independent lattices advanced by one persistent kernel per
+ * sweep phase, replayed as a CUDA graph.  No counterpart in the reference, whose
+ * Lattice<2>::Update holds one static strategy per process (ising/include/lattice.hpp:51-57);
+ * every lattice still sweeps bit-identically to the single-lattice path with the same
+ * extent, tile, lcg width and seeds. ------------------------------------------------------ */
+
+typedef struct swb_batch swb_batch;
+
+/* Creates an empty batch on `device` with room for `capacity` lattices.  hbm_budget_bytes
+ * caps the device memory of all lattices together (0 = no cap).  All lattices of a batch
+ * use lcg32 streams of `lcg_width` lanes. */
+int swb_batch_create(swb_batch **out, uint32_t capacity, uint64_t hbm_budget_bytes, uint32_t lcg_width, int device);
+int swb_batch_destroy(swb_batch *b);
+
+/* Device bytes swb_batch_add would reserve for such a lattice (the admission estimate). */
+int swb_batch_lattice_bytes(uint32_t L0, uint32_t L1, uint32_t tile_x, uint32_t tile_y, uint32_t lcg_width,
+                            uint64_t *bytes);
+
+/* Adds an L0 x L1 lattice with tiles tile_x x tile_y, block_x x block_y tiles per work item
+ * (0 = largest that fits), temperature T and streams seeded seed_base + tile id.  Spins start
+ * all 0; the lattice sweeps without limit until swb_batch_set_schedule.  Fails with
+ * SWB_ERR_CAPACITY when no slot is free or the HBM budget would be exceeded. */
+int swb_batch_add(swb_batch *b, uint32_t L0, uint32_t L1, uint32_t tile_x, uint32_t tile_y, uint32_t block_x,
+                  uint32_t block_y, float temperature, uint32_t seed_base, uint32_t *id);
+int swb_batch_remove(swb_batch *b, uint32_t id);
+
+int swb_batch_hot_start(swb_batch *b, uint32_t id, uint32_t seed);
+int swb_batch_set_spins(swb_batch *b, uint32_t id, const uint8_t *host_spins);
+int swb_batch_get_spins(swb_batch *b, uint32_t id, uint8_t *host_spins);
+int swb_batch_set_temperature(swb_batch *b, uint32_t id, float temperature);
+
+/* Lattice `id` runs `sweeps` more sweeps (0xFFFFFFFF = unlimited) and is measured after every
+ * measure_every-th of its sweeps (0 = never), counted on the device. */
+int swb_batch_set_schedule(swb_batch *b, uint32_t id, uint32_t sweeps, uint32_t measure_every);
+int swb_batch_status(swb_batch *b, uint32_t id, uint32_t *sweeps_left, uint32_t *sweeps_done);
+
+/* n_rounds rounds: every lattice with sweeps left sweeps once per round.  measure != 0 adds
+ * the measurement phase.  Asynchronous (CUDA graph replays on the batch's stream). */
+int swb_batch_sweep(swb_batch *b, uint32_t n_rounds, int measure);
+int swb_batch_synchronize(swb_batch *b);
+
+/* Like swb_batch_sweep without measurement, timed with CUDA events: ms[0] total; with
+ * per_kernel, ms[1..3] = assign, merge, flip kernel time summed over rounds.  Synchronous. */
+int swb_batch_sweep_timed(swb_batch *b, uint32_t n_rounds, int per_kernel, float *ms);
+
+/* Per-lattice observables, as swb_accumulators / swb_samples. */
+int swb_batch_accumulators(swb_batch *b, uint32_t id, double *out);
+int swb_batch_samples(swb_batch *b, uint32_t id, int64_t *em, uint64_t capacity, uint64_t *count);
+int swb_batch_get_rng(swb_batch *b, uint32_t id, uint32_t *state, uint32_t *a, uint32_t *c, uint32_t *iteration);
+
+/* geometry[8] = L0, L1, tile_x, tile_y, tiles per block x, tiles per block y, tiles, blocks. */
+int swb_batch_info(swb_batch *b, uint32_t id, uint32_t *geometry);
+int swb_batch_memory(swb_batch *b, uint64_t *used, uint64_t *budget);
+
+/* One round through HOST spin buffers: copy spins_in[k] to lattice ids[k], sweep every
+ * lattice once, copy the spins back to spins_out[k].  Synchronous. */
+int swb_batch_update_host(swb_batch *b, uint32_t count, const uint32_t *ids, const uint8_t *const *spins_in,
+                          uint8_t *const *spins_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,137 @@
+"""The batched engine: every lattice of a mix is bit-identical to the reference path for its
+extent, tile, lcg width and seeds, whatever else shares the GPU."""
+import numpy as np
+import pytest
+
+from oracle import num_tiles
+
+pytestmark = pytest.mark.gpu
+
+MIX = [
+    # (L0, L1, tile, T, seed_base, block)
+    (64, 64, (16, 8), 2.2691853, 1, (0, 0)),
+    (96, 96, (8, 8), 2.1, 7, (0, 0)),
+    (128, 128, (16, 8), 2.5, 3, (4, 2)),
+    (192, 64, (32, 4), 2.0, 11, (0, 0)),
+    (48, 256, (8, 16), 2.6, 5, (2, 2)),
+    (100, 38, (16, 8), 3.0, 2, (0, 0)),     # ragged tiles
+    (2, 2, (16, 8), 2.2691853, 9, (0, 0)),
+    (512, 512, (16, 8), 2.3, 13, (0, 0)),
+]
+
+
+def _oracle_run(oracle, spins, tile, T, seed, sweeps, W=16):
+    L1, L0 = spins.shape
+    rng = oracle.rng_init(W, num_tiles(L0, L1, *tile), seed)
+    s = spins.copy()
+    for _ in range(sweeps):
+        oracle.sweep(s, tile[0], tile[1], rng, T=T)
+    return s, rng
+
+
+def test_mix_bit_exact(gpu, oracle):
+    rounds = 6
+    with gpu.BatchedSW(capacity=64) as b:
+        ids, starts = [], []
+        for k, (L0, L1, tile, T, seed, block) in enumerate(MIX):
+            i = b.add(L0, L1, T, seed, tile, block)
+            start = oracle.hot_start(L0, L1, 1) if k % 2 == 0 else \
+                np.random.default_rng(k).integers(0, 2, (L1, L0), dtype=np.uint8)
+            b.set_spins(i, start)
+            ids.append(i)
+            starts.append(start)
+        b.sweep(rounds)
+        b.synchronize()
+        for i, start, (L0, L1, tile, T, seed, block) in zip(ids, starts, MIX):
+            want, rng = _oracle_run(oracle, start, tile, T, seed, rounds)
+            assert np.array_equal(b.get_spins(i), want), (L0, L1, tile)
+            st, a, c, it = b.get_rng(i)
+            assert np.array_equal(st, rng.state) and np.array_equal(it, rng.iteration)
+
+
+def test_schedules_and_alone_vs_mix(gpu, oracle):
+    """A lattice with a 3-sweep budget stops after 3 sweeps while the rest continue; the
+    same lattice alone in its own batch ends in the same state."""
+    with gpu.BatchedSW(capacity=16) as mix, gpu.BatchedSW(capacity=2) as alone:
+        a = mix.add(128, 128, 2.2691853, 1, (16, 8))
+        others = [mix.add(L, L, 2.4, 100 + L, (8, 8)) for L in (64, 256, 96)]
+        solo = alone.add(128, 128, 2.2691853, 1, (16, 8))
+        for lid in [a, *others]:
+            mix.hot_start(lid, 1)
+        alone.hot_start(solo, 1)
+        mix.set_schedule(a, 3, 1)
+        alone.set_schedule(solo, 3, 1)
+        mix.sweep(5, measure=True)
+        alone.sweep(3, measure=True)
+        mix.synchronize()
+        assert mix.status(a) == (0, 3)
+        assert mix.status(others[0])[1] == 5
+        got = mix.get_spins(a)
+        assert np.array_equal(got, alone.get_spins(solo))
+        want, _ = _oracle_run(oracle, oracle.hot_start(128, 128, 1), (16, 8), 2.2691853, 1, 3)
+        assert np.array_equal(got, want)
+        s_mix = mix.samples(a)
+        assert np.array_equal(s_mix, alone.samples(solo))
+        assert len(s_mix) == 3
+
+
+def test_measurement_matches_oracle(gpu, oracle):
+    L, T = 96, 2.2691853
+    with gpu.BatchedSW(capacity=4) as b:
+        i = b.add(L, L, T, 1, (16, 8))
+        b.hot_start(i, 1)
+        b.set_schedule(i, 40, 10)
+        b.sweep(40, measure=True)
+        acc = b.accumulators(i)
+        samples = b.samples(i)
+    s = oracle.hot_start(L, L, 1)
+    rng = oracle.rng_init(16, num_tiles(L, L, 16, 8), 1)
+    E = []
+    for k in range(40):
+        oracle.sweep(s, 16, 8, rng, T=T)
+        if (k + 1) % 10 == 0:
+            e, m = oracle.energy_magnetization(s)
+            assert tuple(samples[len(E)]) == (e, m)
+            E.append(-e / (L * L))
+    assert acc[3] == 4 and acc[0] == pytest.approx(sum(E), abs=1e-12)
+
+
+def test_add_remove_between_rounds(gpu, oracle):
+    with gpu.BatchedSW(capacity=8) as b:
+        x = b.add(64, 64, 2.3, 1, (16, 8))
+        b.hot_start(x, 1)
+        b.sweep(2)
+        y = b.add(128, 64, 2.0, 4, (8, 8))
+        b.hot_start(y, 1)
+        b.sweep(3)
+        b.remove(x)
+        b.sweep(2)
+        got_y = b.get_spins(y)
+    want_y, _ = _oracle_run(oracle, oracle.hot_start(128, 64, 1), (8, 8), 2.0, 4, 5)
+    assert np.array_equal(got_y, want_y)
+
+
+def test_hbm_budget_admission(gpu):
+    need = gpu.lattice_bytes(512, 512, (16, 8))
+    with gpu.BatchedSW(capacity=8, hbm_budget_bytes=int(need * 2.5)) as b:
+        b.add(512, 512)
+        b.add(512, 512)
+        with pytest.raises(gpu.NativeError, match="bytes"):
+            b.add(512, 512)
+        used, budget = b.memory()
+        assert used == 2 * need and budget == int(need * 2.5)
+    with gpu.BatchedSW(capacity=1) as b:
+        b.add(64, 64)
+        with pytest.raises(gpu.NativeError, match="slots"):
+            b.add(64, 64)
+
+
+def test_update_host(gpu, oracle):
+    with gpu.BatchedSW(capacity=4) as b:
+        ids = [b.add(64, 64, 2.2, 1, (16, 8)), b.add(128, 96, 2.5, 2, (8, 8))]
+        ins = [oracle.hot_start(64, 64, 1), oracle.hot_start(128, 96, 1)]
+        outs = [np.empty_like(x) for x in ins]
+        b.update_host(ids, ins, outs)
+    for x, o, (tile, T, seed) in zip(ins, outs, [((16, 8), 2.2, 1), ((8, 8), 2.5, 2)]):
+        want, _ = _oracle_run(oracle, x, tile, T, seed, 1)
+        assert np.array_equal(o, want)

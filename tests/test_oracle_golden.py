@@ -1,0 +1,133 @@
+"""Pins the CPU restatement (oracle/sw_oracle.c) against dumps of the unmodified reference
+(tests/golden/, made by tests/golden/make_golden.py from oracle/ref_harness.cpp)."""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import Oracle, num_tiles
+from oracle.exact import KC, exact_energy_heat
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).digest()
+
+
+def case_list(g):
+    return [tuple(c) for c in g["sw_cases"]]
+
+
+@pytest.mark.parametrize("width", [16, 8])
+def test_p_add_bits(oracle, width, golden16, golden8):
+    g = golden16 if width == 16 else golden8
+    got = np.array([oracle.p_add(float(t)) for t in g["p_add_T"]], np.float32)
+    assert np.array_equal(got.view(np.uint32), g["p_add"].view(np.uint32))
+
+
+def test_hot_start(oracle, golden16):
+    assert np.array_equal(oracle.hot_start(64, 32, 1), golden16["hot_start_64x32"])
+    assert sha(oracle.hot_start(1024, 1024, 1)) == golden16["hot_start_1024_sha"].tobytes()
+
+
+@pytest.mark.parametrize("width", [16, 8])
+def test_lcg32_init_and_stream(oracle, width, golden16, golden8):
+    g = golden16 if width == 16 else golden8
+    r = oracle.rng_init(width, len(g["lcg32_seeds"]), seed_base=int(g["lcg32_seeds"][0]))
+    assert np.array_equal(r.state, g["lcg32_state"])
+    assert np.array_equal(r.a, g["lcg32_a"])
+    assert np.array_equal(r.c, g["lcg32_c"])
+    sizes = [int(s) for s in g["next_real_sizes"]]
+    for seed in (1, 7):
+        got = oracle.next_real(width, seed, sizes).view(np.uint32)
+        assert np.array_equal(got, g[f"next_real_seed{seed}"])
+
+
+def _run_case(oracle, g, k, width):
+    L0, L1, tx, ty, T, ns, sb = case_list(g)[k]
+    L0, L1, tx, ty, ns, sb = int(L0), int(L1), int(tx), int(ty), int(ns), int(sb)
+    key = f"sw{k}"
+    if key + "_spins_in" in g:
+        spins = g[key + "_spins_in"].copy()
+    else:
+        seed, kind = (int(x) for x in g[key + "_spins_in_seed"])
+        spins = oracle.hot_start(L0, L1, 1) if kind == 0 else \
+            np.random.default_rng(seed).integers(0, 2, (L1, L0), dtype=np.uint8)
+    rng = oracle.rng_init(width, num_tiles(L0, L1, tx, ty), sb)
+    for s in range(ns):
+        dumps = oracle.sweep(spins, tx, ty, rng, T=float(np.float32(T)), dumps=(s == ns - 1))
+    return key, spins, dumps, rng
+
+
+@pytest.mark.parametrize("width", [16, 8])
+def test_sweep_stages_match_reference(oracle, width, golden16, golden8):
+    g = golden16 if width == 16 else golden8
+    for k in range(len(case_list(g))):
+        key, spins, (bonds, la, lf), rng = _run_case(oracle, g, k, width)
+        if key + "_bonds" in g:
+            assert np.array_equal(bonds, g[key + "_bonds"]), key
+            assert np.array_equal(la, g[key + "_labels_assign"]), key
+            assert np.array_equal(lf, g[key + "_labels_final"]), key
+            assert np.array_equal(spins, g[key + "_spins_out"]), key
+            assert np.array_equal(rng.state, g[key + "_rng_state"]), key
+            assert np.array_equal(rng.a, g[key + "_rng_a"]), key
+            assert np.array_equal(rng.c, g[key + "_rng_c"]), key
+            assert np.array_equal(rng.iteration, g[key + "_rng_iteration"]), key
+        else:
+            for name, arr in (("bonds", bonds), ("labels_assign", la), ("labels_final", lf), ("spins_out", spins),
+                              ("rng_state", rng.state), ("rng_iteration", rng.iteration)):
+                assert sha(arr) == g[key + "_" + name + "_sha"].tobytes(), (key, name)
+        e, m = oracle.energy_magnetization(spins)
+        n = spins.size
+        ref_e, ref_m = g[key + "_em"]
+        assert -e / n == ref_e and m / n == ref_m, key
+
+
+def test_labels_are_canonical_minimum(oracle):
+    L = 96
+    spins = oracle.hot_start(L, L, 1)
+    rng = oracle.rng_init(16, num_tiles(L, L, 16, 8), 1)
+    bonds, la, lf = oracle.sweep(spins, 16, 8, rng, T=2.2691853, dumps=True)
+    idx = np.arange(L * L, dtype=np.uint32).reshape(L, L)
+    assert np.all(lf <= idx) and np.all(la <= idx)
+    flat = lf.ravel()
+    assert np.array_equal(flat[flat], flat)   # every label is a root
+
+
+def test_exact_energy_matches_reference_program():
+    rows = json.load(open(os.path.join(GOLDEN, "exact_ff.json")))
+    for r in rows:
+        e, c = exact_energy_heat(r["K"], r["L"], r["L"])
+        assert abs(e - r["E"]) < 1e-12, r
+        assert abs(c - r["C"]) < 1e-5 * abs(r["C"]), r
+    assert abs(exact_energy_heat(KC, 128)[0] - (-1.419076272084983)) < 1e-12   # README.md:98
+
+
+def test_restatement_reproduces_reference_cli(oracle):
+    """Ising2D (ising/src/ising_2d.cpp) with NUM_THREADS = number of tiles uses one lcg32 stream
+    per tile; the restatement driven the same way prints the same numbers."""
+    runs = json.load(open(os.path.join(GOLDEN, "ising2d_cli.json")))
+    for run in runs:
+        L, sweeps = run["L"], run["num_sweeps"]
+        tx, ty = run["tile"]
+        T = np.float32(2.2691853142130221)
+        spins = oracle.hot_start(L, L, 1)
+        rng = oracle.rng_init(16, num_tiles(L, L, tx, ty), 1)
+        for _ in range(1000):
+            oracle.sweep(spins, tx, ty, rng, T=float(T))
+        E, M = [], []
+        for _ in range(sweeps // 10):
+            for _ in range(10):
+                oracle.sweep(spins, tx, ty, rng, T=float(T))
+            e, m = oracle.energy_magnetization(spins)
+            E.append(-e / (L * L))
+            M.append(abs(m / (L * L)))
+        E = np.array(E)
+        heat = (np.mean(E * E) - E.mean() ** 2) * L * L / (T * T)
+        printed = run["printed"]
+        assert f"{E.mean():g}" == printed["Internal energy per spin"]
+        assert f"{heat:g}" == printed["Heat capacity per spin"]
+        assert f"{np.mean(M):g}" == printed["Absolute Magnetization per spin"]
