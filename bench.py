@@ -356,14 +356,141 @@ def bench_plain(args, dist: Dist, cp) -> dict:
     }
 
 
+def build_mix(cp, device: int, lcg_width: int = 16):
+    from computational_physics_b200 import autotune
+    table = autotune.load(lcg_width=lcg_width)
+    mix = mix_workload()
+    b = cp.BatchedSW(capacity=len(mix), lcg_width=lcg_width, device=device)
+    ids, tiles = [], []
+    for L, T, seed in mix:
+        tile, block = autotune.choice(L, table)
+        lid = b.add(L, L, T, seed, tile, block)
+        b.hot_start(lid, seed)
+        ids.append(lid)
+        tiles.append((tile, block))
+    return b, mix, ids, tiles, table
+
+
+def plain_loop(cp, mix, tiles, steps: int, device: int) -> dict:
+    """The same mix swept by looping the single-lattice path (three launches per lattice per
+    sweep, each lattice on its own stream)."""
+    handles = []
+    for (L, T, seed), (tile, _) in zip(mix, tiles):
+        h = cp.SwendsenWang2D(L, L, tile, 16, seed_base=seed, device=device)
+        h.hot_start(seed)
+        handles.append((h, T))
+    for h, T in handles:
+        h.update(T, 2)
+    for h, _ in handles:
+        h.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for h, T in handles:
+            h.update(T, 1)
+    for h, _ in handles:
+        h.synchronize()
+    secs = time.perf_counter() - t0
+    sites = sum(L * L for L, _, _ in mix)
+    for h, _ in handles:
+        h.close()
+    return {"value": sites * steps / secs, "unit": "spin-updates/s", "steps": steps,
+            "timing": "host wall clock around the loop, all streams synchronized"}
+
+
+def energy_gate(cp, device: int, warmup: int = 1000, sweeps: int = 10000, every: int = 10) -> dict:
+    """Every lattice of the mix: 1000 warmup + 10000 sweeps measured every 10, E/N against the
+    exact finite-lattice value with a binned (autocorrelation-aware) error."""
+    from computational_physics_b200.analysis import gate_energy
+    b, mix, ids, tiles, _ = build_mix(cp, device)
+    b.sweep(warmup)
+    for lid in ids:
+        b.set_schedule(lid, sweeps, every)
+    t0 = time.perf_counter()
+    b.sweep(sweeps, measure=True)
+    b.synchronize()
+    secs = time.perf_counter() - t0
+    z = []
+    worst = None
+    for lid, (L, T, _) in zip(ids, mix):
+        g = gate_energy(b.samples(lid), L, L, T)
+        z.append(g["z"])
+        if worst is None or abs(g["z"]) > abs(worst["z"]):
+            worst = {"L": L, "T": T, **g}
+    b.close()
+    z = np.array(z)
+    return {"lattices": len(z), "within_2sigma": int(np.sum(np.abs(z) <= 2)), "frac_within_2sigma":
+            float(np.mean(np.abs(z) <= 2)), "max_abs_z": float(np.max(np.abs(z))), "mean_z": float(np.mean(z)),
+            "chi2_per_dof": float(np.mean(z * z)), "worst": worst, "seconds": secs,
+            "protocol": f"{warmup} warmup + {sweeps} sweeps, measured every {every}, blocking error"}
+
+
+def bench_batched(args, dist: Dist, cp) -> dict:
+    dev = dist.local_rank
+    b, mix, ids, tiles, table = build_mix(cp, dev)
+    sites = sum(L * L for L, _, _ in mix)
+    b.sweep(args.warmup)
+    b.synchronize()
+    launches0 = cp.kernel_launches()
+    dist.barrier()
+    with ClockSampler(dev) as clocks:
+        ms = float(b.sweep_timed(args.steps)[0])
+    launches = cp.kernel_launches() - launches0
+    dist.barrier()
+    ms_max = dist.max(ms)
+    value = dist.world * sites * args.steps / (ms_max / 1e3)
+    nk = max(3, min(args.steps, 20))
+    k = b.sweep_timed(nk, per_kernel=True)
+    a_ms = float(k[1]) / nk
+    n_tiles = 0
+    for lid in ids:
+        n_tiles += b.info(lid)["tiles"]
+    ab = assign_bytes(sites, n_tiles, 16)
+    peak, peak_kind = hbm_peak()
+    # e2e: every step copies all spins in from pinned host memory and back out
+    ins = []
+    outs = []
+    for lid, (L, _, _) in zip(ids, mix):
+        x = cp.pinned_empty((L, L), np.uint8)
+        x[:] = b.get_spins(lid)
+        ins.append(x)
+        outs.append(cp.pinned_empty((L, L), np.uint8))
+    b.update_host(ids, ins, outs)
+    e2e_steps = max(3, min(args.steps, 10))
+    dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        b.update_host(ids, ins, outs)
+        ins, outs = outs, ins
+    e2e_s = dist.max(time.perf_counter() - t0)
+    b.close()
+    res = {
+        "value": value, "ms_per_step": ms_max / args.steps, "launches": launches, "clocks": clocks.summary(),
+        "roofline": {"bound": "hbm", "kernel": "kb_assign", "achieved": ab / (a_ms / 1e3) / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": ab / (a_ms / 1e3) / 1e9 / peak, "traffic": None, "peak_kind": peak_kind,
+                     "bytes_per_launch": ab, "ms_per_launch": a_ms},
+        "kernels_ms_per_sweep": {"assign": a_ms, "merge": float(k[2]) / nk, "flip": float(k[3]) / nk},
+        "e2e": {"value": dist.world * sites * e2e_steps / e2e_s, "unit": "spin-updates/s",
+                "h2d_bytes_per_step": sites, "d2h_bytes_per_step": sites},
+        "tiles": {str(L): [list(t), list(bl)] for (L, _, _), (t, bl) in sorted(zip(mix, tiles))},
+        "autotune_table": table.get("device", "none"),
+    }
+    if dist.world == 1 and not args.quick:
+        pl = plain_loop(cp, mix, tiles, max(3, min(args.steps, 10)), dev)
+        res["plain_loop"] = pl
+        res["batched_vs_plain_loop"] = value / pl["value"]
+        res["energy_gate"] = energy_gate(cp, dev)
+    return res
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="plain16384", choices=["batched", *PLAIN])
+    ap.add_argument("--workload", default="batched", choices=["batched", *PLAIN])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--quick", action="store_true", help="skip the plain-loop comparison and the energy gate")
     ap.add_argument("--_ref-worker", dest="ref_worker_mode", action="store_true")
     ap.add_argument("--ref-spec", default="")
     args = ap.parse_args()
@@ -379,7 +506,7 @@ def main() -> None:
         import computational_physics_b200 as cp
         if cp.device_count() < 1:
             raise RuntimeError("no CUDA device")
-        r = bench_plain(args, dist, cp)
+        r = bench_batched(args, dist, cp) if args.workload == "batched" else bench_plain(args, dist, cp)
         if dist.rank != 0:
             return
         line = {
@@ -390,6 +517,9 @@ def main() -> None:
             "roofline": r["roofline"], "e2e": r["e2e"], "gpu_launches": r["launches"], "clocks": r["clocks"],
             "kernels_ms_per_sweep": r["kernels_ms_per_sweep"],
         }
+        for key in ("plain_loop", "batched_vs_plain_loop", "energy_gate", "tiles", "autotune_table"):
+            if key in r:
+                line[key] = r[key]
         if dist.world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args.workload)
         print(json.dumps(line))

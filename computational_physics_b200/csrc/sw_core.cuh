@@ -118,6 +118,115 @@ struct LatView {
     float p_add;
 };
 
+// Labelling of a block whose width is a multiple of 32, from the staged spins (sp) and
+// accepted draws (accX, accY, accM) in shared memory.  Warp-per-row: each 32-site word of a
+// row turns into bond bitmasks by __ballot_sync; every site's parent starts at the first site
+// of its x-bonded run (a run's minimum, found with __clz on the gap mask), so horizontal
+// bonds need no union; a vertical bond is united only when the bond to its left does not
+// already join the same two runs.  The result equals the generic path's: the minimum site
+// index of each block-local component.
+__device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uint32_t bxi, const uint32_t byi,
+                                                         uint32_t *__restrict__ labels, uint32_t *__restrict__ edge,
+                                                         unsigned char *smem)
+{
+    const AssignSmem L = assign_smem(g);
+    uint32_t *parent = reinterpret_cast<uint32_t *>(smem + L.parent);
+    const uint64_t *accM = reinterpret_cast<const uint64_t *>(smem + L.accM);
+    const uint32_t *accX = reinterpret_cast<const uint32_t *>(smem + L.accX);
+    const uint32_t *accY = reinterpret_cast<const uint32_t *>(smem + L.accY);
+    uint32_t *edge_s = reinterpret_cast<uint32_t *>(smem + L.edge);
+    const uint8_t *sp = smem + L.sp;
+    const uint32_t BX = g.BX, BY = g.BY, NW = BX >> 5;
+    uint32_t *Xw = reinterpret_cast<uint32_t *>(smem + L.bond);  // [BY][NW] x-bonds inside the block
+    uint32_t *Yw = Xw + BY * NW;                                  // [BY][NW] y-bonds inside the block
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    const uint32_t x0 = bxi * BX, y0 = byi * BY;
+    const uint32_t bxv = min(BX, g.L0 - x0), byv = min(BY, g.L1 - y0);
+    const uint32_t pitch = L.pitch;
+    const uint32_t txs = 31 - __clz(g.TX);  // TX is 8, 16 or 32
+
+    // bond words; edge bonds go to edge_s (right edge: one bit per row, bottom: the row's words)
+    for (uint32_t yl = warp; yl < BY; yl += nwarps) {
+        const uint32_t tby = yl / g.TY, jj = yl - tby * g.TY;
+        const uint32_t jjmax = byv > tby * g.TY ? min(g.TY, byv - tby * g.TY) : 0;
+        for (uint32_t w = 0; w < NW; ++w) {
+            const uint32_t xl = (w << 5) + lane;
+            bool xb = false, yb = false;
+            if (xl < bxv && yl < byv) {
+                const uint32_t tbx = xl >> txs, tb = tby * g.TBX + tbx;
+                const uint32_t ii = xl - (tbx << txs);
+                const uint32_t iimax = min(g.TX, bxv - (tbx << txs));
+                const uint8_t s = sp[yl * pitch + xl];
+                const uint32_t xa = (ii + 1 < iimax) ? (accX[tb * g.TY + jj] >> ii) : (uint32_t)(accM[tb] >> (g.TX + jj));
+                const uint32_t ya = (jj + 1 < jjmax) ? (accY[tb * g.TY + jj] >> ii) : (uint32_t)(accM[tb] >> ii);
+                xb = (xa & 1u) && s == sp[yl * pitch + xl + 1];
+                yb = (ya & 1u) && s == sp[(yl + 1) * pitch + xl];
+            }
+            uint32_t X = __ballot_sync(0xffffffffu, xb), Y = __ballot_sync(0xffffffffu, yb);
+            if (lane == 0) {
+                if (bxv - 1 - (w << 5) < 32u) {  // the block's last column lies in this word
+                    const uint32_t bit = (bxv - 1) & 31;
+                    if ((X >> bit) & 1u)
+                        atomicOr(edge_s, 1u << yl);
+                    X &= ~(1u << bit);
+                }
+                if (yl + 1 == byv) {
+                    edge_s[1 + w] = Y;
+                    Y = 0;
+                }
+                Xw[yl * NW + w] = X;
+                Yw[yl * NW + w] = Y;
+            }
+        }
+    }
+    __syncthreads();
+
+    // parent = first site of the x-bonded run
+    for (uint32_t yl = warp; yl < BY; yl += nwarps) {
+        uint32_t carry = 0, carry_on = 0;
+        for (uint32_t w = 0; w < NW; ++w) {
+            const uint32_t X = Xw[yl * NW + w];
+            const uint32_t gaps = ~X & ((1u << lane) - 1u);
+            const uint32_t start = gaps ? (w << 5) + 32 - __clz(gaps) : (carry_on ? carry : (w << 5));
+            parent[yl * BX + (w << 5) + lane] = yl * BX + start;
+            carry = __shfl_sync(0xffffffffu, start, 31);
+            carry_on = X >> 31;
+        }
+    }
+    __syncthreads();
+
+    // vertical bonds, skipping those whose left neighbour already joins the same two runs
+    for (uint32_t yl = warp; yl + 1 < BY; yl += nwarps) {
+        uint32_t prev = 0;
+        for (uint32_t w = 0; w < NW; ++w) {
+            const uint32_t Y = Yw[yl * NW + w];
+            const uint32_t X = Xw[yl * NW + w], Xb = Xw[(yl + 1) * NW + w];
+            const uint32_t T = Y & X & Xb;
+            const uint32_t U = Y & ~((T << 1) | prev);
+            prev = T >> 31;
+            if ((U >> lane) & 1u) {
+                const uint32_t l = yl * BX + (w << 5) + lane;
+                uf_union(parent, l, l + BX);
+            }
+        }
+    }
+    __syncthreads();
+
+    // block-local minimum as a global site index
+    for (uint32_t yl = warp; yl < byv; yl += nwarps) {
+        uint32_t *row = labels + (size_t)(y0 + yl) * g.L0 + x0;
+        for (uint32_t w = 0; w < NW; ++w) {
+            const uint32_t xl = (w << 5) + lane;
+            if (xl < bxv) {
+                const uint32_t r = uf_find(parent, yl * BX + xl);
+                row[xl] = (y0 + r / BX) * g.L0 + x0 + (r & (BX - 1));
+            }
+        }
+    }
+    if (tid < kEdgeWords)
+        edge[((size_t)byi * g.nbx + bxi) * kEdgeWords + tid] = edge_s[tid];
+}
+
 // Block (bxi, byi) of a lattice: lcg32 draws, bonds, union-find in shared memory.  Runs on
 // all threads of the CTA (at least TBX * TBY * W of them); smem holds assign_smem(g).total bytes.
 template <int W>
@@ -245,6 +354,11 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
             accM[tb] = mbits;
     }
     __syncthreads();
+
+    if (dbg_assign == nullptr && (BX & 31u) == 0 && (BX & (BX - 1)) == 0) {
+        assign_block_labels_rows(g, bxi, byi, labels, edge, smem);
+        return;
+    }
 
     // ---- 3. bonds (bit 0 +x, bit 1 +y): equal spins and an accepted draw.  The last
     // column / row of a tile bonds through the merge draw: [0, TX) bottom, [TX, TX+TY) right.

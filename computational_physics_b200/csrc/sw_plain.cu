@@ -404,7 +404,7 @@ int swb_create(swb_lattice **out, uint32_t L0, uint32_t L1, uint32_t tile_x, uin
     SWB_TRY(cudaMalloc(&h->rng_iter, (size_t)h->n_tiles * sizeof(uint32_t)));
     SWB_TRY(cudaMalloc(&h->edge, (size_t)h->n_blocks * kEdgeWords * sizeof(uint32_t)));
     SWB_TRY(cudaMalloc(&h->obs, sizeof(Obs)));
-    h->series_cap = 1ull << 20;
+    h->series_cap = 1ull << 17;  // 131072 measurements (2 MiB)
     SWB_TRY(cudaMalloc(&h->series, h->series_cap * 2 * sizeof(long long)));
     SWB_TRY(cudaMalloc(&h->scratch_flag, sizeof(unsigned int)));
     SWB_TRY(cudaMemsetAsync(h->spins, 0, h->n + 16, h->stream));
