@@ -20,6 +20,7 @@ extra_signatures({
     "swb_batch_set_temperature": ([P, U32, F32], I32),
     "swb_batch_set_schedule": ([P, U32, U32, U32], I32),
     "swb_batch_status": ([P, U32, P, P], I32),
+    "swb_batch_poll": ([P, P, P], I32),
     "swb_batch_sweep": ([P, U32, I32], I32),
     "swb_batch_synchronize": ([P], I32),
     "swb_batch_sweep_timed": ([P, U32, I32, P], I32),
@@ -56,6 +57,7 @@ class BatchedSW:
         h = ctypes.c_void_p()
         check(self._lib.swb_batch_create(ctypes.byref(h), capacity, hbm_budget_bytes, lcg_width, device))
         self._h = h
+        self.capacity = capacity
         self.lcg_width = lcg_width
         self.shapes: dict[int, tuple[int, int]] = {}
 
@@ -114,6 +116,13 @@ class BatchedSW:
         done = ctypes.c_uint32()
         check(self._lib.swb_batch_status(self._h, lid, ctypes.byref(left), ctypes.byref(done)))
         return left.value, done.value
+
+    def poll(self) -> tuple[np.ndarray, np.ndarray]:
+        """sweeps_left and sweeps_done of every slot (0 for free slots)."""
+        left = np.zeros(self.capacity, np.uint32)
+        done = np.zeros(self.capacity, np.uint32)
+        check(self._lib.swb_batch_poll(self._h, _ptr(left), _ptr(done)))
+        return left, done
 
     def sweep(self, rounds: int = 1, measure: bool = False) -> None:
         check(self._lib.swb_batch_sweep(self._h, rounds, int(measure)))

@@ -3,8 +3,8 @@
 //
 // Work queue.  Every active lattice contributes its blocks (TBX x TBY tiles) to one flat list
 // of work items; a lattice's items follow the exclusive prefix sum blk_prefix.  The persistent
-// CTAs of kb_assign / kb_merge pull items from a device counter (atomicAdd) until the list is
-// exhausted; kb_flip and kb_measure do the same over chunks of 4096 sites.  Each phase resets
+// CTAs of kb_assign / kb_merge / kb_flip pull items from a device counter (atomicAdd) until the
+// list is exhausted; kb_measure does the same over chunks of 4096 sites.  Each phase resets
 // the counter of the phase that ran before it, so a sweep needs no host work and the whole
 // sweep is one CUDA graph, captured once per handle and replayed: the graph reads the item
 // totals from device memory, so adding or removing lattices does not invalidate it.
@@ -27,7 +27,7 @@
 namespace swb {
 
 constexpr uint32_t kBatchThreads = 512;        // CTA size of the persistent kernels
-constexpr uint32_t kChunkSites = 4096;         // flip / measure work item
+constexpr uint32_t kChunkSites = 4096;         // measure work item
 constexpr uint32_t kUnlimited = 0xFFFFFFFFu;   // sweeps_left value that never runs out
 
 struct BatchLat {
@@ -46,7 +46,7 @@ struct BatchLat {
     uint32_t swept;           // 1 if this lattice was swept in the current round
     uint32_t measure_every;   // measure after every measure_every-th sweep (0: never)
     uint32_t sweeps_done;     // sweeps completed
-    uint32_t chunks_left;     // flip chunks not yet done in this round
+    uint32_t blocks_left;     // flip work items not yet done in this round
 };
 
 struct BatchCounters {
@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(kBatchThreads) kb_assign(BatchLat *lats, const
 }
 
 __global__ void __launch_bounds__(kBatchThreads) kb_merge(BatchLat *lats, const uint32_t *active, const uint32_t *blk_prefix,
-                                                          BatchCounters *ctr)
+                                                          BatchCounters *ctr, unsigned int *fault)
 {
     __shared__ uint32_t slot;
     if (blockIdx.x == 0 && threadIdx.x == 0)
@@ -125,50 +125,36 @@ __global__ void __launch_bounds__(kBatchThreads) kb_merge(BatchLat *lats, const 
             continue;
         const Geo g = L->g;
         if (threadIdx.x < g.BX + g.BY)
-            merge_block(g, item - blk_prefix[k], threadIdx.x, L->edge, L->labels);
+            merge_block(g, item - blk_prefix[k], threadIdx.x, L->edge, L->labels, fault);
     }
 }
 
-// Resolve + flip of one chunk; the last chunk of a lattice closes its round (sweep budget).
-__global__ void __launch_bounds__(kBatchThreads) kb_flip(BatchLat *lats, const uint32_t *active, const uint32_t *chunk_prefix,
-                                                         BatchCounters *ctr)
+// Resolve + flip of one block (flip_block); the last block of a lattice closes its round
+// (sweep count and budget).
+__global__ void __launch_bounds__(kBatchThreads) kb_flip(BatchLat *lats, const uint32_t *active, const uint32_t *blk_prefix,
+                                                         BatchCounters *ctr, unsigned int *fault)
 {
+    extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint32_t slot;
     if (blockIdx.x == 0 && threadIdx.x == 0)
         ctr->queue[1] = 0;
-    const uint32_t n = ctr->n_active, total = ctr->total_chunks;
+    const uint32_t n = ctr->n_active, total = ctr->total_blocks;
     while (true) {
         const uint32_t item = next_item(&ctr->queue[2], &slot);
         if (item >= total)
             break;
-        const uint32_t k = find_lattice(chunk_prefix, n, item);
+        const uint32_t k = find_lattice(blk_prefix, n, item);
         BatchLat *L = lats + active[k];
         if (L->sweeps_left == 0)
             continue;
-        const size_t nsites = (size_t)L->g.L0 * L->g.L1;
-        const size_t q0 = (size_t)(item - chunk_prefix[k]) * (kChunkSites / 4);
-        const size_t q1 = min(q0 + kChunkSites / 4, nsites / 4);
-        const uint32_t *labels = L->labels;
-        for (size_t q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
-            const uint4 lab = reinterpret_cast<const uint4 *>(labels)[q];
-            const uint32_t r[4] = {lab.x, lab.y, lab.z, lab.w};
-            uint32_t flip = 0;
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                uint32_t c = r[j], d;
-                while ((d = labels[c]) != c)
-                    c = d;
-                flip |= (c & 1u) << (8 * j);
-            }
-            reinterpret_cast<uint32_t *>(L->spins)[q] ^= flip;
-        }
+        const Geo g = L->g;
+        const uint32_t blk = item - blk_prefix[k];
+        flip_block<false>(g, blk % g.nbx, blk / g.nbx, L->spins, L->labels, fault, smem);
         __syncthreads();
         if (threadIdx.x == 0) {
             __threadfence();
-            if (atomicSub(&L->chunks_left, 1u) == 1u) {
-                // last chunk of this lattice in this round
-                const uint32_t nchunks = chunk_prefix[k + 1] - chunk_prefix[k];
-                L->chunks_left = nchunks;
+            if (atomicSub(&L->blocks_left, 1u) == 1u) {
+                L->blocks_left = g.nbx * g.nby;
                 L->swept = 1;
                 L->sweeps_done += 1;
                 if (L->sweeps_left != kUnlimited)
@@ -329,10 +315,11 @@ struct swb_batch {
     BatchLat *d_lats = nullptr;
     uint32_t *d_active = nullptr, *d_blk_prefix = nullptr, *d_chunk_prefix = nullptr;
     BatchCounters *d_ctr = nullptr;
+    unsigned int *d_fault = nullptr;
     std::vector<uint32_t> active;   // ids in the work lists
     bool lists_dirty = true;
-    int grid_assign = 0, grid_other = 0;
-    uint32_t smem_assign = 0;
+    int grid_assign = 0, grid_other = 0, grid_flip = 0;
+    uint32_t smem_assign = 0, smem_flip = 0;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};   // [measure?]
     uint64_t series_cap = 1u << 16;
 };
@@ -342,6 +329,17 @@ namespace {
 int bset_device(const swb_batch *b)
 {
     SWB_CUDA(cudaSetDevice(b->device));
+    return SWB_OK;
+}
+
+// Non-zero fault word: a label chase ran past kChainCap steps (only corrupt labels can).
+int bcheck_fault(swb_batch *b)
+{
+    unsigned int f = 0;
+    SWB_CUDA(cudaMemcpyAsync(&f, b->d_fault, sizeof(f), cudaMemcpyDeviceToHost, b->stream));
+    SWB_CUDA(cudaStreamSynchronize(b->stream));
+    if (f)
+        return fail(SWB_ERR_STATE, "label chase exceeded %u steps (fault word %u)", kChainCap, f);
     return SWB_OK;
 }
 
@@ -405,9 +403,11 @@ int launch_round_w(swb_batch *b, bool measure)
     kb_assign<W><<<b->grid_assign, kBatchThreads, b->smem_assign, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix,
                                                                               b->d_ctr);
     SWB_LAUNCHED();
-    kb_merge<<<b->grid_other, kBatchThreads, 0, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix, b->d_ctr);
+    kb_merge<<<b->grid_other, kBatchThreads, 0, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix, b->d_ctr,
+                                                             b->d_fault);
     SWB_LAUNCHED();
-    kb_flip<<<b->grid_other, kBatchThreads, 0, b->stream>>>(b->d_lats, b->d_active, b->d_chunk_prefix, b->d_ctr);
+    kb_flip<<<b->grid_flip, kBatchThreads, b->smem_flip, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix, b->d_ctr,
+                                                                      b->d_fault);
     SWB_LAUNCHED();
     if (measure) {
         kb_measure<<<b->grid_other, kBatchThreads, 0, b->stream>>>(b->d_lats, b->d_active, b->d_chunk_prefix,
@@ -517,6 +517,8 @@ int swb_batch_create(swb_batch **out, uint32_t capacity, uint64_t hbm_budget_byt
     SWB_TRY(cudaMalloc(&b->d_blk_prefix, 4 * (capacity + 1)));
     SWB_TRY(cudaMalloc(&b->d_chunk_prefix, 4 * (capacity + 1)));
     SWB_TRY(cudaMalloc(&b->d_ctr, sizeof(BatchCounters)));
+    SWB_TRY(cudaMalloc(&b->d_fault, sizeof(unsigned int)));
+    SWB_TRY(cudaMemsetAsync(b->d_fault, 0, sizeof(unsigned int), b->stream));
     SWB_TRY(cudaMemsetAsync(b->d_ctr, 0, sizeof(BatchCounters), b->stream));
     SWB_TRY(cudaMemsetAsync(b->d_blk_prefix, 0, 4 * (capacity + 1), b->stream));
     SWB_TRY(cudaMemsetAsync(b->d_chunk_prefix, 0, 4 * (capacity + 1), b->stream));
@@ -532,9 +534,12 @@ int swb_batch_create(swb_batch **out, uint32_t capacity, uint64_t hbm_budget_byt
     default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kb_assign<32>, kBatchThreads, b->smem_assign); break;
     }
     b->grid_assign = sms * std::max(per_sm, 1);
-    int per_sm2 = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, kb_flip, kBatchThreads, 0);
+    b->smem_flip = flip_smem_bytes(gmax);
+    int per_sm2 = 1, per_sm3 = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, kb_merge, kBatchThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm3, kb_flip, kBatchThreads, b->smem_flip);
     b->grid_other = sms * std::max(per_sm2, 1);
+    b->grid_flip = sms * std::max(per_sm3, 1);
     SWB_TRY(cudaStreamSynchronize(b->stream));
 #undef SWB_TRY
     *out = b;
@@ -559,6 +564,7 @@ int swb_batch_destroy(swb_batch *b)
     cudaFree(b->d_blk_prefix);
     cudaFree(b->d_chunk_prefix);
     cudaFree(b->d_ctr);
+    cudaFree(b->d_fault);
     if (b->stream)
         cudaStreamDestroy(b->stream);
     delete b;
@@ -615,7 +621,7 @@ int swb_batch_add(swb_batch *b, uint32_t L0, uint32_t L1, uint32_t tile_x, uint3
     d.p_add = swb_p_add(temperature);
     d.sweeps_left = kUnlimited;
     d.measure_every = 0;
-    d.chunks_left = lattice_chunks(g);
+    d.blocks_left = g.nbx * g.nby;
     SWB_CUDA(cudaMemsetAsync(d.spins, 0, n, b->stream));
     SWB_CUDA(cudaMemsetAsync(d.obs, 0, sizeof(Obs), b->stream));
     switch (b->W) {
@@ -689,7 +695,7 @@ int swb_batch_get_spins(swb_batch *b, uint32_t id, uint8_t *host_spins)
         return rc;
     SWB_CUDA(cudaMemcpyAsync(host_spins, h->d.spins, (size_t)h->d.g.L0 * h->d.g.L1, cudaMemcpyDeviceToHost, b->stream));
     SWB_CUDA(cudaStreamSynchronize(b->stream));
-    return SWB_OK;
+    return bcheck_fault(b);
 }
 
 int swb_batch_set_temperature(swb_batch *b, uint32_t id, float temperature)
@@ -738,6 +744,24 @@ int swb_batch_status(swb_batch *b, uint32_t id, uint32_t *sweeps_left, uint32_t 
     return SWB_OK;
 }
 
+int swb_batch_poll(swb_batch *b, uint32_t *sweeps_left, uint32_t *sweeps_done)
+{
+    if (!b || !sweeps_left)
+        return fail(SWB_ERR_ARGUMENT, "NULL argument");
+    if (int rc = bset_device(b))
+        return rc;
+    std::vector<BatchLat> d(b->capacity);
+    SWB_CUDA(cudaMemcpyAsync(d.data(), b->d_lats, sizeof(BatchLat) * b->capacity, cudaMemcpyDeviceToHost, b->stream));
+    SWB_CUDA(cudaStreamSynchronize(b->stream));
+    for (uint32_t i = 0; i < b->capacity; ++i) {
+        const bool used = b->lats[i].used;
+        sweeps_left[i] = used ? d[i].sweeps_left : 0;
+        if (sweeps_done)
+            sweeps_done[i] = used ? d[i].sweeps_done : 0;
+    }
+    return SWB_OK;
+}
+
 int swb_batch_sweep(swb_batch *b, uint32_t n_rounds, int measure)
 {
     if (!b)
@@ -754,7 +778,7 @@ int swb_batch_synchronize(swb_batch *b)
     if (int rc = bset_device(b))
         return rc;
     SWB_CUDA(cudaStreamSynchronize(b->stream));
-    return SWB_OK;
+    return bcheck_fault(b);
 }
 
 int swb_batch_sweep_timed(swb_batch *b, uint32_t n_rounds, int per_kernel, float *ms)
@@ -785,10 +809,12 @@ int swb_batch_sweep_timed(swb_batch *b, uint32_t n_rounds, int per_kernel, float
             }
             SWB_LAUNCHED();
             SWB_CUDA(cudaEventRecord(ev[2], b->stream));
-            kb_merge<<<b->grid_other, kBatchThreads, 0, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix, b->d_ctr);
+            kb_merge<<<b->grid_other, kBatchThreads, 0, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix, b->d_ctr,
+                                                                     b->d_fault);
             SWB_LAUNCHED();
             SWB_CUDA(cudaEventRecord(ev[3], b->stream));
-            kb_flip<<<b->grid_other, kBatchThreads, 0, b->stream>>>(b->d_lats, b->d_active, b->d_chunk_prefix, b->d_ctr);
+            kb_flip<<<b->grid_flip, kBatchThreads, b->smem_flip, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix,
+                                                                              b->d_ctr, b->d_fault);
             SWB_LAUNCHED();
             SWB_CUDA(cudaEventRecord(ev[4], b->stream));
             SWB_CUDA(cudaEventSynchronize(ev[4]));
@@ -806,7 +832,7 @@ int swb_batch_sweep_timed(swb_batch *b, uint32_t n_rounds, int per_kernel, float
     SWB_CUDA(cudaEventElapsedTime(&ms[0], ev[0], ev[4]));
     for (auto &e : ev)
         cudaEventDestroy(e);
-    return rc;
+    return rc ? rc : bcheck_fault(b);
 }
 
 int swb_batch_accumulators(swb_batch *b, uint32_t id, double *out)

@@ -446,7 +446,7 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
 // Unions across the right and bottom edge (periodic) of block blk: thread t < BY takes row
 // t of the right edge, BY <= t < BY + BX column t - BY of the bottom edge.
 __device__ __forceinline__ void merge_block(const Geo &g, const uint32_t blk, const uint32_t t,
-                                            const uint32_t *__restrict__ edge, uint32_t *labels)
+                                            const uint32_t *__restrict__ edge, uint32_t *labels, unsigned int *fault)
 {
     const uint32_t bxi = blk % g.nbx, byi = blk / g.nbx;
     const uint32_t x0 = bxi * g.BX, y0 = byi * g.BY;
@@ -472,7 +472,100 @@ __device__ __forceinline__ void merge_block(const Geo &g, const uint32_t blk, co
         const volatile uint32_t *vl = labels;
         const uint32_t a = vl[s], b = vl[nb];
         if (a != b)
-            uf_union(labels, a, b);
+            guf_union(labels, a, b, fault);
+    }
+}
+
+// Shared memory of flip_block: the resolved root of every referenced block-local site and a
+// bitmap of which sites are referenced.
+__host__ __device__ inline uint32_t flip_smem_bytes(const Geo &g)
+{
+    return g.BX * g.BY * 4 + ((g.BX * g.BY + 31) / 32) * 4;
+}
+
+// ResolveLabels + FlipClusters for block (bxi, byi) after the merge.  A site's label is its
+// block-local root (k_assign) unless the site is itself a root that the merge linked onward.
+// Every distinct label that lies in the block is resolved once (guf_find, which also
+// compresses the chain for the other blocks); each site then takes its root's result from
+// shared memory and flips iff the cluster's label is odd.  kWriteLabels stores the resolved
+// labels (the reference's ResolveLabels output).
+template <bool kWriteLabels>
+__device__ __forceinline__ void flip_block(const Geo &g, const uint32_t bxi, const uint32_t byi, uint8_t *spins,
+                                           uint32_t *labels, unsigned int *fault, unsigned char *smem)
+{
+    const uint32_t BX = g.BX, BY = g.BY, NS = BX * BY, L0 = g.L0;
+    uint32_t *res = reinterpret_cast<uint32_t *>(smem);
+    uint32_t *need = res + NS;
+    const uint32_t tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
+    const uint32_t x0 = bxi * BX, y0 = byi * BY;
+    const uint32_t bxv = min(BX, L0 - x0), byv = min(BY, g.L1 - y0);
+    const uint32_t base = y0 * L0 + x0, span = byv * L0;
+    const float inv = 1.0f / (float)L0;
+    // Block-local index of label v, or NS when v lies outside the block.
+    auto local = [&](uint32_t v) -> uint32_t {
+        const uint32_t d = v - base;
+        if (d >= span)
+            return NS;
+        uint32_t yl = __float2uint_rz((float)d * inv);
+        if (yl * L0 > d)
+            --yl;
+        else if ((yl + 1) * L0 <= d)
+            ++yl;
+        const uint32_t xl = d - yl * L0;
+        return xl < bxv ? yl * BX + xl : NS;
+    };
+    for (uint32_t i = tid; i < (NS + 31) / 32; i += nthr)
+        need[i] = 0;
+    __syncthreads();
+    for (uint32_t yl = warp; yl < byv; yl += nwarps)
+        for (uint32_t xl = lane; xl < bxv; xl += 32) {
+            const uint32_t lv = local(labels[base + yl * L0 + xl]);
+            if (lv < NS)
+                atomicOr(need + (lv >> 5), 1u << (lv & 31));
+        }
+    __syncthreads();
+    for (uint32_t yl = warp; yl < byv; yl += nwarps)
+        for (uint32_t xl = lane; xl < bxv; xl += 32) {
+            const uint32_t l = yl * BX + xl;
+            if ((need[l >> 5] >> (l & 31)) & 1u)
+                res[l] = guf_find(labels, base + yl * L0 + xl, fault);
+        }
+    __syncthreads();
+    // A root's label may have been compressed by another CTA since the first pass: trust res
+    // only for sites whose result was computed, resolve anything else directly.
+    auto resolve = [&](uint32_t v) -> uint32_t {
+        const uint32_t lv = local(v);
+        if (lv < NS && ((need[lv >> 5] >> (lv & 31)) & 1u))
+            return res[lv];
+        return guf_find(labels, v, fault);
+    };
+    const bool quads = (L0 & 3u) == 0;
+    for (uint32_t yl = warp; yl < byv; yl += nwarps) {
+        const uint32_t row = base + yl * L0;
+        if (quads) {
+            for (uint32_t q = lane; 4 * q < bxv; q += 32) {
+                const uint32_t s = row + 4 * q;
+                const uint4 lab = *reinterpret_cast<const uint4 *>(labels + s);
+                const uint32_t v[4] = {lab.x, lab.y, lab.z, lab.w};
+                uint32_t r[4], flip = 0;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    r[k] = resolve(v[k]);
+                    flip |= (r[k] & 1u) << (8 * k);
+                }
+                reinterpret_cast<uint32_t *>(spins)[s >> 2] ^= flip;
+                if (kWriteLabels)
+                    *reinterpret_cast<uint4 *>(labels + s) = make_uint4(r[0], r[1], r[2], r[3]);
+            }
+        } else {
+            for (uint32_t xl = lane; xl < bxv; xl += 32) {
+                const uint32_t s = row + xl;
+                const uint32_t r = resolve(labels[s]);
+                spins[s] ^= (uint8_t)(r & 1u);
+                if (kWriteLabels)
+                    labels[s] = r;
+            }
+        }
     }
 }
 

@@ -100,4 +100,51 @@ __device__ __forceinline__ void uf_union(uint32_t *p, uint32_t a, uint32_t b)
     }
 }
 
+// ---- the same on the global label array, which other CTAs change concurrently.  Finds halve
+// the path as they go (x's parent becomes its grandparent); the update is an atomicMin, which
+// only ever moves a pointer to an ancestor, so it is safe against concurrent unions and keeps
+// the trees shallow.  Every loop is capped: parents strictly decrease, so a chain longer than
+// kChainCap means corrupt labels; the walk then stops and raises *fault.
+constexpr uint32_t kChainCap = 1u << 22;
+constexpr uint32_t kUnionRetryCap = 1u << 16;
+
+__device__ __forceinline__ uint32_t guf_find(uint32_t *p, uint32_t x, unsigned int *fault)
+{
+    const volatile uint32_t *vp = p;
+    uint32_t y = vp[x];
+    for (uint32_t n = 0; y != x; ++n) {
+        const uint32_t z = vp[y];
+        if (z == y)
+            return y;
+        if (n >= kChainCap) {
+            atomicOr(fault, 1u);
+            return y;
+        }
+        atomicMin(p + x, z);  // path halving
+        x = z;
+        y = vp[x];
+    }
+    return x;
+}
+
+__device__ __forceinline__ void guf_union(uint32_t *p, uint32_t a, uint32_t b, unsigned int *fault)
+{
+    for (uint32_t n = 0; n < kUnionRetryCap; ++n) {
+        a = guf_find(p, a, fault);
+        b = guf_find(p, b, fault);
+        if (a == b)
+            return;
+        if (a > b) {
+            const uint32_t t = a;
+            a = b;
+            b = t;
+        }
+        const uint32_t old = atomicMin(p + b, a);
+        if (old == b)
+            return;
+        b = old;
+    }
+    atomicOr(fault, 2u);
+}
+
 }  // namespace swb

@@ -71,55 +71,21 @@ __global__ void __launch_bounds__(1024) k_assign(const Geo g, const uint8_t *__r
                     dbg_assign, smem);
 }
 
-__global__ void __launch_bounds__(256) k_merge(const Geo g, const uint32_t *__restrict__ edge, uint32_t *labels)
+__global__ void __launch_bounds__(256) k_merge(const Geo g, const uint32_t *__restrict__ edge, uint32_t *labels,
+                                               unsigned int *fault)
 {
-    merge_block(g, blockIdx.x, threadIdx.x, edge, labels);
+    merge_block(g, blockIdx.x, threadIdx.x, edge, labels, fault);
 }
 
-// Root of each site's label chain; spin ^= root & 1.  Optionally writes the root back
-// (the reference's ResolveLabels result).
+// Resolve + flip, one CTA per block (flip_block).
+constexpr uint32_t kFlipThreads = 512;
+
 template <bool kWriteLabels>
-__global__ void __launch_bounds__(256) k_flip(const uint32_t n, uint8_t *__restrict__ spins, uint32_t *labels)
+__global__ void __launch_bounds__(kFlipThreads) k_flip(const Geo g, uint8_t *__restrict__ spins, uint32_t *labels,
+                                                       unsigned int *fault)
 {
-    const volatile uint32_t *vl = labels;
-    const size_t stride = (size_t)gridDim.x * blockDim.x;
-    if ((n & 3u) == 0) {
-        const size_t nq = n >> 2;
-        for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += stride) {
-            uint4 lab;
-            if (kWriteLabels) {
-                lab.x = vl[4 * q]; lab.y = vl[4 * q + 1]; lab.z = vl[4 * q + 2]; lab.w = vl[4 * q + 3];
-            } else {
-                lab = reinterpret_cast<const uint4 *>(labels)[q];
-            }
-            uint32_t r[4] = {lab.x, lab.y, lab.z, lab.w};
-            uint32_t flip = 0;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                uint32_t c = r[k], d;
-                if (kWriteLabels) {
-                    while ((d = vl[c]) != c) c = d;
-                } else {
-                    while ((d = labels[c]) != c) c = d;
-                }
-                r[k] = c;
-                flip |= (c & 1u) << (8 * k);
-            }
-            uint32_t *sw = reinterpret_cast<uint32_t *>(spins) + q;
-            *sw ^= flip;
-            if (kWriteLabels) {
-                labels[4 * q] = r[0]; labels[4 * q + 1] = r[1]; labels[4 * q + 2] = r[2]; labels[4 * q + 3] = r[3];
-            }
-        }
-    } else {
-        for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-            uint32_t c = vl[i], d;
-            while ((d = vl[c]) != c) c = d;
-            spins[i] ^= (uint8_t)(c & 1u);
-            if (kWriteLabels)
-                labels[i] = c;
-        }
-    }
+    extern __shared__ __align__(16) unsigned char smem[];
+    flip_block<kWriteLabels>(g, blockIdx.x, blockIdx.y, spins, labels, fault, smem);
 }
 
 __global__ void __launch_bounds__(256) k_measure(const uint32_t L0, const uint32_t L1, const uint8_t *__restrict__ spins,
@@ -266,12 +232,13 @@ struct swb_lattice {
     long long *series = nullptr;
     unsigned long long series_cap = 0;
     unsigned int *scratch_flag = nullptr;
-    int flip_grid = 0, measure_grid = 0;
+    unsigned int *fault = nullptr;  // set by a chase that exceeded kChainCap
+    int measure_grid = 0;
+    uint32_t smem_flip = 0;
 };
 
 namespace {
 
-const uint32_t kFlipThreads = 256;
 
 int set_device(const swb_lattice *h)
 {
@@ -283,7 +250,8 @@ template <int W>
 int launch_assign_w(swb_lattice *h, float p_add, uint8_t *dbg_bonds, uint32_t *dbg_assign)
 {
     const Geo &g = h->g;
-    const dim3 grid(g.nbx, g.nby), block(g.TBX * g.TBY * W);
+    // Whole warps: the draws use full-warp shuffles and ballots; surplus lanes have no tile.
+    const dim3 grid(g.nbx, g.nby), block((g.TBX * g.TBY * W + 31) / 32 * 32);
     k_assign<W><<<grid, block, h->smem_assign, h->stream>>>(g, h->spins, h->labels, h->rng_state, h->rng_sel,
                                                             h->rng_iter, p_add, h->edge, dbg_bonds, dbg_assign);
     SWB_LAUNCHED();
@@ -305,12 +273,12 @@ int launch_sweep(swb_lattice *h, float p_add, bool write_labels, uint8_t *dbg_bo
     int rc = launch_assign(h, p_add, dbg_bonds, dbg_assign);
     if (rc)
         return rc;
-    k_merge<<<h->n_blocks, h->g.BX + h->g.BY, 0, h->stream>>>(h->g, h->edge, h->labels);
+    k_merge<<<h->n_blocks, h->g.BX + h->g.BY, 0, h->stream>>>(h->g, h->edge, h->labels, h->fault);
     SWB_LAUNCHED();
     if (write_labels)
-        k_flip<true><<<h->flip_grid, kFlipThreads, 0, h->stream>>>((uint32_t)h->n, h->spins, h->labels);
+        k_flip<true><<<dim3(h->g.nbx, h->g.nby), kFlipThreads, h->smem_flip, h->stream>>>(h->g, h->spins, h->labels, h->fault);
     else
-        k_flip<false><<<h->flip_grid, kFlipThreads, 0, h->stream>>>((uint32_t)h->n, h->spins, h->labels);
+        k_flip<false><<<dim3(h->g.nbx, h->g.nby), kFlipThreads, h->smem_flip, h->stream>>>(h->g, h->spins, h->labels, h->fault);
     SWB_LAUNCHED();
     return SWB_OK;
 }
@@ -324,6 +292,18 @@ int launch_measure(swb_lattice *h, int accumulate)
 }
 
 bool valid_width(uint32_t W) { return W == 8 || W == 16 || W == 32; }
+
+// Reads the device fault word (after the handle's work so far); non-zero means a label chase
+// ran past kChainCap steps, which only corrupt labels can cause.
+int check_fault(swb_lattice *h)
+{
+    unsigned int f = 0;
+    SWB_CUDA(cudaMemcpyAsync(&f, h->fault, sizeof(f), cudaMemcpyDeviceToHost, h->stream));
+    SWB_CUDA(cudaStreamSynchronize(h->stream));
+    if (f)
+        return fail(SWB_ERR_STATE, "label chase exceeded %u steps (fault word %u)", kChainCap, f);
+    return SWB_OK;
+}
 
 int index_of_pair(uint32_t a, uint32_t c)
 {
@@ -407,12 +387,12 @@ int swb_create(swb_lattice **out, uint32_t L0, uint32_t L1, uint32_t tile_x, uin
     h->series_cap = 1ull << 17;  // 131072 measurements (2 MiB)
     SWB_TRY(cudaMalloc(&h->series, h->series_cap * 2 * sizeof(long long)));
     SWB_TRY(cudaMalloc(&h->scratch_flag, sizeof(unsigned int)));
+    SWB_TRY(cudaMalloc(&h->fault, sizeof(unsigned int)));
+    SWB_TRY(cudaMemsetAsync(h->fault, 0, sizeof(unsigned int), h->stream));
     SWB_TRY(cudaMemsetAsync(h->spins, 0, h->n + 16, h->stream));
     SWB_TRY(cudaMemsetAsync(h->obs, 0, sizeof(Obs), h->stream));
-    const size_t nq = (h->n % 4 == 0) ? h->n / 4 : h->n;
-    h->flip_grid = (int)std::min<size_t>((nq + kFlipThreads - 1) / kFlipThreads, (size_t)sms * 16);
+    h->smem_flip = flip_smem_bytes(h->g);
     h->measure_grid = (int)std::min<size_t>((h->n + 255) / 256, (size_t)sms * 8);
-    if (h->flip_grid < 1) h->flip_grid = 1;
     if (h->measure_grid < 1) h->measure_grid = 1;
     switch (h->W) {
     case 8: k_rng_init<8><<<(h->n_tiles + 127) / 128, 128, 0, h->stream>>>(h->n_tiles, seed_base, h->rng_state, h->rng_sel, h->rng_iter); break;
@@ -443,6 +423,7 @@ int swb_destroy(swb_lattice *h)
     cudaFree(h->obs);
     cudaFree(h->series);
     cudaFree(h->scratch_flag);
+    cudaFree(h->fault);
     if (h->stream)
         cudaStreamDestroy(h->stream);
     delete h;
@@ -475,7 +456,7 @@ int swb_get_spins(swb_lattice *h, uint8_t *host_spins)
         return rc;
     SWB_CUDA(cudaMemcpyAsync(host_spins, h->spins, h->n, cudaMemcpyDeviceToHost, h->stream));
     SWB_CUDA(cudaStreamSynchronize(h->stream));
-    return SWB_OK;
+    return check_fault(h);
 }
 
 int swb_hot_start(swb_lattice *h, uint32_t seed)
@@ -545,7 +526,7 @@ int swb_sweep_recorded(swb_lattice *h, float temperature, uint8_t *bonds, uint32
     cudaFreeAsync(d_bonds, h->stream);
     cudaFreeAsync(d_assign, h->stream);
     SWB_CUDA(cudaStreamSynchronize(h->stream));
-    return rc;
+    return rc ? rc : check_fault(h);
 }
 
 int swb_synchronize(swb_lattice *h)
@@ -555,7 +536,7 @@ int swb_synchronize(swb_lattice *h)
     if (int rc = set_device(h))
         return rc;
     SWB_CUDA(cudaStreamSynchronize(h->stream));
-    return SWB_OK;
+    return check_fault(h);
 }
 
 int swb_energy_magnetization(swb_lattice *h, double *out, int64_t *e_sum, int64_t *m_sum)
@@ -712,10 +693,10 @@ int swb_sweep_timed(swb_lattice *h, float temperature, uint32_t n_sweeps, int pe
         if ((rc = launch_assign(h, p_add, nullptr, nullptr)))
             break;
         SWB_CUDA(cudaEventRecord(ev[2], h->stream));
-        k_merge<<<h->n_blocks, h->g.BX + h->g.BY, 0, h->stream>>>(h->g, h->edge, h->labels);
+        k_merge<<<h->n_blocks, h->g.BX + h->g.BY, 0, h->stream>>>(h->g, h->edge, h->labels, h->fault);
         SWB_LAUNCHED();
         SWB_CUDA(cudaEventRecord(ev[3], h->stream));
-        k_flip<false><<<h->flip_grid, kFlipThreads, 0, h->stream>>>((uint32_t)h->n, h->spins, h->labels);
+        k_flip<false><<<dim3(h->g.nbx, h->g.nby), kFlipThreads, h->smem_flip, h->stream>>>(h->g, h->spins, h->labels, h->fault);
         SWB_LAUNCHED();
         SWB_CUDA(cudaEventRecord(ev[4], h->stream));
         SWB_CUDA(cudaEventSynchronize(ev[4]));
@@ -732,7 +713,7 @@ int swb_sweep_timed(swb_lattice *h, float temperature, uint32_t n_sweeps, int pe
     SWB_CUDA(cudaEventElapsedTime(&ms[0], ev[0], ev[4]));
     for (auto &e : ev)
         cudaEventDestroy(e);
-    return rc;
+    return rc ? rc : check_fault(h);
 }
 
 int swb_host_alloc(void **ptr, size_t bytes)

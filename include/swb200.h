@@ -176,6 +176,10 @@ int swb_batch_set_temperature(swb_batch *b, uint32_t id, float temperature);
 int swb_batch_set_schedule(swb_batch *b, uint32_t id, uint32_t sweeps, uint32_t measure_every);
 int swb_batch_status(swb_batch *b, uint32_t id, uint32_t *sweeps_left, uint32_t *sweeps_done);
 
+/* sweeps_left / sweeps_done (may be NULL) of every slot, arrays of `capacity` entries (0 for
+ * free slots), in one device-to-host copy.  Synchronous. */
+int swb_batch_poll(swb_batch *b, uint32_t *sweeps_left, uint32_t *sweeps_done);
+
 /* n_rounds rounds: every lattice with sweeps left sweeps once per round.  measure != 0 adds
  * the measurement phase.  Asynchronous (CUDA graph replays on the batch's stream). */
 int swb_batch_sweep(swb_batch *b, uint32_t n_rounds, int measure);
