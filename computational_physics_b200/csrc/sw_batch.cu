@@ -82,7 +82,7 @@ __device__ __forceinline__ uint32_t next_item(unsigned int *queue, uint32_t *slo
 }
 
 template <int W>
-__global__ void __launch_bounds__(kBatchThreads) kb_assign(BatchLat *lats, const uint32_t *active, const uint32_t *blk_prefix,
+__global__ void __launch_bounds__(kBatchThreads, 4) kb_assign(BatchLat *lats, const uint32_t *active, const uint32_t *blk_prefix,
                                                            BatchCounters *ctr)
 {
     extern __shared__ __align__(16) unsigned char smem[];

@@ -144,6 +144,7 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
     const uint32_t bxv = min(BX, g.L0 - x0), byv = min(BY, g.L1 - y0);
     const uint32_t pitch = L.pitch;
     const uint32_t txs = 31 - __clz(g.TX);  // TX is 8, 16 or 32
+    const uint32_t bxs = 31 - __clz(BX);     // BX is a power of two on this path
 
     // bond words; edge bonds go to edge_s (right edge: one bit per row, bottom: the row's words)
     for (uint32_t yl = warp; yl < BY; yl += nwarps) {
@@ -219,7 +220,7 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
             const uint32_t xl = (w << 5) + lane;
             if (xl < bxv) {
                 const uint32_t r = uf_find(parent, yl * BX + xl);
-                row[xl] = (y0 + r / BX) * g.L0 + x0 + (r & (BX - 1));
+                row[xl] = (y0 + (r >> bxs)) * g.L0 + x0 + (r & (BX - 1));
             }
         }
     }
@@ -252,8 +253,8 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
     const uint32_t bxv = min(BX, g.L0 - x0), byv = min(BY, g.L1 - y0);
     const uint32_t pitch = L.pitch;
 
-    for (uint32_t i = tid; i < ntb * g.TY * 2 + kEdgeWords; i += nthr)
-        accX[i] = 0;  // accX, accY and edge_s are contiguous
+    if (tid < kEdgeWords)
+        edge_s[tid] = 0;
 
     // ---- 1. spins of the block and its halo (column x0+bxv and row y0+byv, periodic)
     {
@@ -293,17 +294,14 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
         uint32_t a = lcg_param_a(sel), c = lcg_param_c(sel);
         const uint32_t Ur = (g.TX + W - 1) / W, Um = (g.TX + g.TY + W - 1) / W;
         const uint32_t nrow = on ? 2 * jjmax - 1 : 0;
-        const uint32_t rowU = nrow * Ur, myU = on ? rowU + Um : 0;
-        const uint32_t maxU = (2 * g.TY - 1) * Ur + Um;
         const uint32_t seg_shift = ((tid & 31) / W) * W;
-        uint64_t mbits = 0;
-        for (uint32_t u = 0; u < maxU; ++u) {
-            const bool upd = u < myU;
+        const uint32_t seg_mask = (W == 32) ? 0xffffffffu : ((1u << (W & 31)) - 1u);
+        // One LCG32_State::Update of every lane of the tile (random/src/lcg32.cpp:162-195): on
+        // every 15th the (a, c) pairs first rotate by state[it & (W-1)] + (it odd ? 0 : 1).
+        auto advance = [&](const bool upd) {
             const uint32_t itn = it + 1;
             const bool rot = upd && (itn % kShuffleDistance) == 0;
             if (__any_sync(0xffffffffu, rot)) {
-                // Parameter rotation of random/src/lcg32.cpp:168-188: lane i takes the pair of
-                // lane (i + state[it & (W-1)] + (it odd ? 0 : 1)) & (W-1), before stepping.
                 const uint32_t src = __shfl_sync(0xffffffffu, st, itn & (W - 1), W);
                 const uint32_t from = (lane + src + ((itn & 1u) ? 0u : 1u)) & (W - 1);
                 const uint32_t a2 = __shfl_sync(0xffffffffu, a, from, W);
@@ -315,34 +313,35 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
                     sel = s2;
                 }
             }
-            bool bit = false, is_row = false;
-            uint32_t req = 0, sub = 0;
             if (upd) {
                 it = itn;
                 st = a * st + c;
-                if (u < rowU) {
-                    req = u / Ur;
-                    sub = u - req * Ur;
-                    is_row = true;
-                    bit = sub * W + lane < g.TX && lcg_accept(st, p_add);
-                } else {
-                    sub = u - rowU;
-                    bit = sub * W + lane < g.TX + g.TY && lcg_accept(st, p_add);
-                }
             }
-            const uint32_t m = __ballot_sync(0xffffffffu, bit);
-            const uint32_t seg = (W == 32) ? m : ((m >> seg_shift) & ((1u << (W & 31)) - 1u));
-            if (lane == 0 && upd) {
-                if (is_row) {
-                    const uint32_t word = seg << (sub * W);
-                    if (req < jjmax)
-                        accX[tb * g.TY + req] |= word;
-                    else
-                        accY[tb * g.TY + req - jjmax] |= word;
-                } else {
-                    mbits |= (uint64_t)seg << (sub * W);
-                }
+        };
+        // Row requests: tile_x numbers each, x-bond rows then y-bond rows; element k is lane
+        // k % W after update k / W + 1 of the request.  The ballot gives every lane the whole
+        // word; one lane stores it.
+        for (uint32_t req = 0; req < 2 * g.TY - 1; ++req) {
+            const bool upd = req < nrow;
+            uint32_t word = 0;
+            for (uint32_t sub = 0; sub < Ur; ++sub) {
+                advance(upd);
+                const bool bit = upd && sub * W + lane < g.TX && lcg_accept(st, p_add);
+                word |= ((__ballot_sync(0xffffffffu, bit) >> seg_shift) & seg_mask) << (sub * W);
             }
+            if (upd && lane == (req & (W - 1))) {
+                if (req < jjmax)
+                    accX[tb * g.TY + req] = word;
+                else
+                    accY[tb * g.TY + req - jjmax] = word;
+            }
+        }
+        // The merge request: tile_x + tile_y numbers, [0, tile_x) bottom edge, then right edge.
+        uint64_t mbits = 0;
+        for (uint32_t sub = 0; sub < Um; ++sub) {
+            advance(on);
+            const bool bit = on && sub * W + lane < g.TX + g.TY && lcg_accept(st, p_add);
+            mbits |= (uint64_t)((__ballot_sync(0xffffffffu, bit) >> seg_shift) & seg_mask) << (sub * W);
         }
         if (on) {
             rng_state[(size_t)tile * W + lane] = st;

@@ -59,8 +59,10 @@ int fail(int code, const char *fmt, ...)
     return code;
 }
 
+constexpr uint32_t kAssignThreads = 512;  // at most this many lcg lanes per block
+
 template <int W>
-__global__ void __launch_bounds__(1024) k_assign(const Geo g, const uint8_t *__restrict__ spins,
+__global__ void __launch_bounds__(kAssignThreads, 4) k_assign(const Geo g, const uint8_t *__restrict__ spins,
                                                  uint32_t *__restrict__ labels, uint32_t *__restrict__ rng_state,
                                                  uint8_t *__restrict__ rng_sel, uint32_t *__restrict__ rng_iter,
                                                  const float p_add, uint32_t *__restrict__ edge,
@@ -356,7 +358,7 @@ int swb_create(swb_lattice **out, uint32_t L0, uint32_t L1, uint32_t tile_x, uin
     h->device = device;
     h->W = lcg_width;
     h->seed_base = seed_base;
-    h->g = make_geo(L0, L1, tile_x, tile_y, lcg_width);
+    h->g = make_geo(L0, L1, tile_x, tile_y, lcg_width, kAssignThreads);
     h->n = (size_t)L0 * L1;
     h->n_tiles = h->g.n0 * h->g.n1;
     h->n_blocks = h->g.nbx * h->g.nby;
