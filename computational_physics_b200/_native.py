@@ -42,6 +42,7 @@ _SIGNATURES = {
     "swb_hot_start": ([P, U32], I32),
     "swb_cold_start": ([P, ctypes.c_uint8], I32),
     "swb_p_add": ([F32], F32),
+    "swb_accept_threshold": ([F32], U32),
     "swb_sweep": ([P, F32, U32, U32], I32),
     "swb_sweep_recorded": ([P, F32, P, P, P], I32),
     "swb_synchronize": ([P], I32),

@@ -41,7 +41,7 @@ struct BatchLat {
     Obs *obs;
     long long *series;
     unsigned long long series_cap;
-    float p_add;
+    uint32_t thr;             // bond accept threshold, accept_threshold(p_add)
     uint32_t sweeps_left;     // sweeps still to run (kUnlimited: no limit)
     uint32_t swept;           // 1 if this lattice was swept in the current round
     uint32_t measure_every;   // measure after every measure_every-th sweep (0: never)
@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4) kb_assign(BatchLat *lats, co
         const Geo g = L->g;
         const uint32_t blk = item - blk_prefix[k];
         assign_block<W>(g, blk % g.nbx, blk / g.nbx, L->spins, L->labels, L->rng_state, L->rng_sel, L->rng_iter,
-                        L->p_add, L->edge, nullptr, nullptr, smem);
+                        L->thr, L->edge, nullptr, nullptr, smem);
         __syncthreads();
     }
 }
@@ -578,8 +578,8 @@ int swb_batch_add(swb_batch *b, uint32_t L0, uint32_t L1, uint32_t tile_x, uint3
         return fail(SWB_ERR_ARGUMENT, "NULL argument");
     if (L0 == 0 || L1 == 0 || (L0 % 2) || (L1 % 2))
         return fail(SWB_ERR_ARGUMENT, "SwendsenWang_2D implementation requires evenly sized lattice (%u x %u)", L0, L1);
-    if ((uint64_t)L0 * L1 > 0xFFFFFFFFull)
-        return fail(SWB_ERR_ARGUMENT, "lattice of %u x %u sites exceeds 32-bit labels", L0, L1);
+    if ((uint64_t)L0 * L1 > 0x7FFFFFFFull)
+        return fail(SWB_ERR_ARGUMENT, "lattice of %u x %u sites exceeds 2^31 - 1 labels", L0, L1);
     if (!(tile_x == 8 || tile_x == 16 || tile_x == 32) || tile_y < 2 || tile_y > 32)
         return fail(SWB_ERR_ARGUMENT, "unsupported tile %u x %u", tile_x, tile_y);
     if (!(temperature > 0.0f) || !std::isfinite(temperature))
@@ -618,7 +618,7 @@ int swb_batch_add(swb_batch *b, uint32_t L0, uint32_t L1, uint32_t tile_x, uint3
     d.obs = reinterpret_cast<Obs *>(p); p += al(sizeof(Obs));
     d.series = reinterpret_cast<long long *>(p);
     d.series_cap = b->series_cap;
-    d.p_add = swb_p_add(temperature);
+    d.thr = accept_threshold(swb_p_add(temperature));
     d.sweeps_left = kUnlimited;
     d.measure_every = 0;
     d.blocks_left = g.nbx * g.nby;
@@ -707,8 +707,8 @@ int swb_batch_set_temperature(swb_batch *b, uint32_t id, float temperature)
         return fail(SWB_ERR_ARGUMENT, "temperature must be positive and finite");
     if (int rc = bset_device(b))
         return rc;
-    h->d.p_add = swb_p_add(temperature);
-    SWB_CUDA(cudaMemcpyAsync(&b->d_lats[id].p_add, &h->d.p_add, sizeof(float), cudaMemcpyHostToDevice, b->stream));
+    h->d.thr = accept_threshold(swb_p_add(temperature));
+    SWB_CUDA(cudaMemcpyAsync(&b->d_lats[id].thr, &h->d.thr, sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream));
     SWB_CUDA(cudaStreamSynchronize(b->stream));
     return SWB_OK;
 }

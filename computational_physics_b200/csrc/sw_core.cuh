@@ -82,6 +82,23 @@ inline Geo make_geo(uint32_t L0, uint32_t L1, uint32_t TX, uint32_t TY, uint32_t
 
 constexpr uint32_t kEdgeWords = 8;  // per block: [0] right edge rows, [1..4] bottom edge columns
 
+// Label encoding between the assign and flip phases of a sweep.  A block root holds its global
+// site index (< 2^31); these are the only entries the merge reads and links.  Every other site
+// holds kLocalFlag | the block-local index (yl * BX + xl) of its root, which needs no division
+// to resolve and marks the site as a non-root.  Resolved labels (global) are written only by a
+// recorded sweep.
+constexpr uint32_t kLocalFlag = 0x80000000u;
+constexpr uint32_t kLocalMask = 0x0000FFFFu;
+
+// Global site index of a label read at a site of block (bxi, byi).
+__device__ __forceinline__ uint32_t label_global(const Geo &g, uint32_t bxi, uint32_t byi, uint32_t v)
+{
+    if (!(v & kLocalFlag))
+        return v;
+    const uint32_t r = v & kLocalMask;
+    return (byi * g.BY + r / g.BX) * g.L0 + bxi * g.BX + r % g.BX;
+}
+
 struct AssignSmem {
     uint32_t parent, accM, accX, accY, edge, bond, sp, total, pitch;
 };
@@ -115,7 +132,7 @@ struct LatView {
     uint8_t *rng_sel;
     uint32_t *rng_iter;
     uint32_t *edge;
-    float p_add;
+    uint32_t thr;  // bond accept threshold, accept_threshold(p_add)
 };
 
 // Labelling of a block whose width is a multiple of 32, from the staged spins (sp) and
@@ -144,7 +161,6 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
     const uint32_t bxv = min(BX, g.L0 - x0), byv = min(BY, g.L1 - y0);
     const uint32_t pitch = L.pitch;
     const uint32_t txs = 31 - __clz(g.TX);  // TX is 8, 16 or 32
-    const uint32_t bxs = 31 - __clz(BX);     // BX is a power of two on this path
 
     // bond words; edge bonds go to edge_s (right edge: one bit per row, bottom: the row's words)
     for (uint32_t yl = warp; yl < BY; yl += nwarps) {
@@ -213,14 +229,28 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
     }
     __syncthreads();
 
-    // block-local minimum as a global site index
+    // Roots of the runs: every run's first site follows its chain once and points straight at
+    // the block root; afterwards any site's root is parent[parent[site]] (its run start's).
+    for (uint32_t yl = warp; yl < BY; yl += nwarps)
+        for (uint32_t w = 0; w < NW; ++w) {
+            const uint32_t left = lane ? (Xw[yl * NW + w] >> (lane - 1)) & 1u : (w ? Xw[yl * NW + w - 1] >> 31 : 0u);
+            if (!left) {
+                const uint32_t l = yl * BX + (w << 5) + lane;
+                parent[l] = uf_find(parent, l);
+            }
+        }
+    __syncthreads();
+
+    // Labels: a block root stores its global site index (the merge links these), every other
+    // site kLocalFlag | the block-local index of its root.
     for (uint32_t yl = warp; yl < byv; yl += nwarps) {
         uint32_t *row = labels + (size_t)(y0 + yl) * g.L0 + x0;
         for (uint32_t w = 0; w < NW; ++w) {
             const uint32_t xl = (w << 5) + lane;
             if (xl < bxv) {
-                const uint32_t r = uf_find(parent, yl * BX + xl);
-                row[xl] = (y0 + (r >> bxs)) * g.L0 + x0 + (r & (BX - 1));
+                const uint32_t l = yl * BX + xl;
+                const uint32_t r = parent[parent[l]];
+                row[xl] = r == l ? (y0 + yl) * g.L0 + x0 + xl : (kLocalFlag | r);
             }
         }
     }
@@ -234,7 +264,7 @@ template <int W>
 __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, const uint32_t byi,
                                              const uint8_t *__restrict__ spins, uint32_t *__restrict__ labels,
                                              uint32_t *__restrict__ rng_state, uint8_t *__restrict__ rng_sel,
-                                             uint32_t *__restrict__ rng_iter, const float p_add,
+                                             uint32_t *__restrict__ rng_iter, const uint32_t thr,
                                              uint32_t *__restrict__ edge, uint8_t *__restrict__ dbg_bonds,
                                              uint32_t *__restrict__ dbg_assign, unsigned char *smem)
 {
@@ -292,6 +322,7 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
             it = rng_iter[tile];
         }
         uint32_t a = lcg_param_a(sel), c = lcg_param_c(sel);
+        uint32_t to_rot = kShuffleDistance - it % kShuffleDistance;  // updates until the next rotation
         const uint32_t Ur = (g.TX + W - 1) / W, Um = (g.TX + g.TY + W - 1) / W;
         const uint32_t nrow = on ? 2 * jjmax - 1 : 0;
         const uint32_t seg_shift = ((tid & 31) / W) * W;
@@ -300,7 +331,7 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
         // every 15th the (a, c) pairs first rotate by state[it & (W-1)] + (it odd ? 0 : 1).
         auto advance = [&](const bool upd) {
             const uint32_t itn = it + 1;
-            const bool rot = upd && (itn % kShuffleDistance) == 0;
+            const bool rot = upd && to_rot == 1;
             if (__any_sync(0xffffffffu, rot)) {
                 const uint32_t src = __shfl_sync(0xffffffffu, st, itn & (W - 1), W);
                 const uint32_t from = (lane + src + ((itn & 1u) ? 0u : 1u)) & (W - 1);
@@ -316,6 +347,7 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
             if (upd) {
                 it = itn;
                 st = a * st + c;
+                to_rot = rot ? kShuffleDistance : to_rot - 1;
             }
         };
         // Row requests: tile_x numbers each, x-bond rows then y-bond rows; element k is lane
@@ -326,7 +358,7 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
             uint32_t word = 0;
             for (uint32_t sub = 0; sub < Ur; ++sub) {
                 advance(upd);
-                const bool bit = upd && sub * W + lane < g.TX && lcg_accept(st, p_add);
+                const bool bit = upd && sub * W + lane < g.TX && lcg_accept(st, thr);
                 word |= ((__ballot_sync(0xffffffffu, bit) >> seg_shift) & seg_mask) << (sub * W);
             }
             if (upd && lane == (req & (W - 1))) {
@@ -340,7 +372,7 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
         uint64_t mbits = 0;
         for (uint32_t sub = 0; sub < Um; ++sub) {
             advance(on);
-            const bool bit = on && sub * W + lane < g.TX + g.TY && lcg_accept(st, p_add);
+            const bool bit = on && sub * W + lane < g.TX + g.TY && lcg_accept(st, thr);
             mbits |= (uint64_t)((__ballot_sync(0xffffffffu, bit) >> seg_shift) & seg_mask) << (sub * W);
         }
         if (on) {
@@ -430,12 +462,13 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
     }
     __syncthreads();
 
-    // ---- 6. block-local minimum as a global site index
+    // ---- 6. labels: a block root stores its global site index, every other site
+    // kLocalFlag | the block-local index of its root
     for (uint32_t l = tid; l < NS; l += nthr) {
         const uint32_t xl = l % BX, yl = l / BX;
         if (xl < bxv && yl < byv) {
             const uint32_t r = uf_find(parent, l);
-            labels[(size_t)(y0 + yl) * g.L0 + x0 + xl] = (y0 + r / BX) * g.L0 + x0 + r % BX;
+            labels[(size_t)(y0 + yl) * g.L0 + x0 + xl] = r == l ? (y0 + yl) * g.L0 + x0 + xl : (kLocalFlag | r);
         }
     }
     if (tid < kEdgeWords)
@@ -452,11 +485,13 @@ __device__ __forceinline__ void merge_block(const Geo &g, const uint32_t blk, co
     const uint32_t bxv = min(g.BX, g.L0 - x0), byv = min(g.BY, g.L1 - y0);
     const uint32_t *e = edge + (size_t)blk * kEdgeWords;
     size_t s = 0, nb = 0;
+    uint32_t nbx = bxi, nby = byi;  // block of the neighbour site
     bool go = false;
     if (t < g.BY) {
         if (t < byv && ((e[0] >> t) & 1u)) {
             s = (size_t)(y0 + t) * g.L0 + x0 + bxv - 1;
             nb = (size_t)(y0 + t) * g.L0 + (x0 + bxv) % g.L0;
+            nbx = bxi + 1 == g.nbx ? 0 : bxi + 1;
             go = true;
         }
     } else {
@@ -464,84 +499,49 @@ __device__ __forceinline__ void merge_block(const Geo &g, const uint32_t blk, co
         if (xl < bxv && ((e[1 + (xl >> 5)] >> (xl & 31)) & 1u)) {
             s = (size_t)(y0 + byv - 1) * g.L0 + x0 + xl;
             nb = (size_t)((y0 + byv) % g.L1) * g.L0 + x0 + xl;
+            nby = byi + 1 == g.nby ? 0 : byi + 1;
             go = true;
         }
     }
     if (go) {
         const volatile uint32_t *vl = labels;
-        const uint32_t a = vl[s], b = vl[nb];
+        const uint32_t a = label_global(g, bxi, byi, vl[s]), b = label_global(g, nbx, nby, vl[nb]);
         if (a != b)
             guf_union(labels, a, b, fault);
     }
 }
 
-// Shared memory of flip_block: the resolved root of every referenced block-local site and a
-// bitmap of which sites are referenced.
+// Shared memory of flip_block: the resolved label of every block root.
 __host__ __device__ inline uint32_t flip_smem_bytes(const Geo &g)
 {
-    return g.BX * g.BY * 4 + ((g.BX * g.BY + 31) / 32) * 4;
+    return g.BX * g.BY * 4;
 }
 
-// ResolveLabels + FlipClusters for block (bxi, byi) after the merge.  A site's label is its
-// block-local root (k_assign) unless the site is itself a root that the merge linked onward.
-// Every distinct label that lies in the block is resolved once (guf_find, which also
-// compresses the chain for the other blocks); each site then takes its root's result from
-// shared memory and flips iff the cluster's label is odd.  kWriteLabels stores the resolved
-// labels (the reference's ResolveLabels output).
+// ResolveLabels + FlipClusters for block (bxi, byi) after the merge.  Block roots (labels
+// without kLocalFlag) follow their chain once (guf_find, which also compresses it for the other
+// blocks) into shared memory; every site then reads its root's result there and flips iff the
+// cluster's label is odd.  kWriteLabels stores the resolved global labels (the reference's
+// ResolveLabels output).
 template <bool kWriteLabels>
 __device__ __forceinline__ void flip_block(const Geo &g, const uint32_t bxi, const uint32_t byi, uint8_t *spins,
                                            uint32_t *labels, unsigned int *fault, unsigned char *smem)
 {
-    const uint32_t BX = g.BX, BY = g.BY, NS = BX * BY, L0 = g.L0;
+    const uint32_t BX = g.BX, L0 = g.L0;
     uint32_t *res = reinterpret_cast<uint32_t *>(smem);
-    uint32_t *need = res + NS;
-    const uint32_t tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
-    const uint32_t x0 = bxi * BX, y0 = byi * BY;
-    const uint32_t bxv = min(BX, L0 - x0), byv = min(BY, g.L1 - y0);
-    const uint32_t base = y0 * L0 + x0, span = byv * L0;
-    const float inv = 1.0f / (float)L0;
-    // Block-local index of label v, or NS when v lies outside the block.
-    auto local = [&](uint32_t v) -> uint32_t {
-        const uint32_t d = v - base;
-        if (d >= span)
-            return NS;
-        uint32_t yl = __float2uint_rz((float)d * inv);
-        if (yl * L0 > d)
-            --yl;
-        else if ((yl + 1) * L0 <= d)
-            ++yl;
-        const uint32_t xl = d - yl * L0;
-        return xl < bxv ? yl * BX + xl : NS;
-    };
-    for (uint32_t i = tid; i < (NS + 31) / 32; i += nthr)
-        need[i] = 0;
-    __syncthreads();
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    const uint32_t x0 = bxi * BX, y0 = byi * g.BY;
+    const uint32_t bxv = min(BX, L0 - x0), byv = min(g.BY, g.L1 - y0);
+    const uint32_t base = y0 * L0 + x0;
     for (uint32_t yl = warp; yl < byv; yl += nwarps)
         for (uint32_t xl = lane; xl < bxv; xl += 32) {
-            const uint32_t lv = local(labels[base + yl * L0 + xl]);
-            if (lv < NS)
-                atomicOr(need + (lv >> 5), 1u << (lv & 31));
+            const uint32_t site = base + yl * L0 + xl;
+            if (!(labels[site] & kLocalFlag))
+                res[yl * BX + xl] = guf_find(labels, site, fault);
         }
     __syncthreads();
-    for (uint32_t yl = warp; yl < byv; yl += nwarps)
-        for (uint32_t xl = lane; xl < bxv; xl += 32) {
-            const uint32_t l = yl * BX + xl;
-            if ((need[l >> 5] >> (l & 31)) & 1u)
-                res[l] = guf_find(labels, base + yl * L0 + xl, fault);
-        }
-    __syncthreads();
-    // A root's label may have been compressed by another CTA since the first pass: trust res
-    // only for sites whose result was computed, resolve anything else directly.
-    auto resolve = [&](uint32_t v) -> uint32_t {
-        const uint32_t lv = local(v);
-        if (lv < NS && ((need[lv >> 5] >> (lv & 31)) & 1u))
-            return res[lv];
-        return guf_find(labels, v, fault);
-    };
-    const bool quads = (L0 & 3u) == 0;
-    for (uint32_t yl = warp; yl < byv; yl += nwarps) {
-        const uint32_t row = base + yl * L0;
-        if (quads) {
+    if ((L0 & 3u) == 0) {
+        for (uint32_t yl = warp; yl < byv; yl += nwarps) {
+            const uint32_t row = base + yl * L0;
             for (uint32_t q = lane; 4 * q < bxv; q += 32) {
                 const uint32_t s = row + 4 * q;
                 const uint4 lab = *reinterpret_cast<const uint4 *>(labels + s);
@@ -549,22 +549,24 @@ __device__ __forceinline__ void flip_block(const Geo &g, const uint32_t bxi, con
                 uint32_t r[4], flip = 0;
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
-                    r[k] = resolve(v[k]);
+                    r[k] = res[(v[k] & kLocalFlag) ? (v[k] & kLocalMask) : yl * BX + 4 * q + k];
                     flip |= (r[k] & 1u) << (8 * k);
                 }
                 reinterpret_cast<uint32_t *>(spins)[s >> 2] ^= flip;
                 if (kWriteLabels)
                     *reinterpret_cast<uint4 *>(labels + s) = make_uint4(r[0], r[1], r[2], r[3]);
             }
-        } else {
+        }
+    } else {
+        for (uint32_t yl = warp; yl < byv; yl += nwarps)
             for (uint32_t xl = lane; xl < bxv; xl += 32) {
-                const uint32_t s = row + xl;
-                const uint32_t r = resolve(labels[s]);
+                const uint32_t s = base + yl * L0 + xl;
+                const uint32_t v = labels[s];
+                const uint32_t r = res[(v & kLocalFlag) ? (v & kLocalMask) : yl * BX + xl];
                 spins[s] ^= (uint8_t)(r & 1u);
                 if (kWriteLabels)
                     labels[s] = r;
             }
-        }
     }
 }
 

@@ -25,11 +25,29 @@ __host__ __device__ __forceinline__ uint32_t lcg_param_c(uint32_t sel)
 constexpr uint32_t kShuffleDistance = 15;          // LCG32_State::ShuffleDistance (lcg32.hpp:43)
 constexpr float kTwoPowMinus32 = 2.3283064365386963e-10f;  // the float the reference's literal rounds to
 
-// Accept test of the bond draw: (float)u * 2^-32 < p_add with u rounded to nearest
-// (random/src/lcg32.cpp:231-240 and the '< p_add' of the callers).
-__device__ __forceinline__ bool lcg_accept(uint32_t u, float p_add)
+// Accept test of a bond draw.  The reference accepts when (float)u * 2^-32 < p_add, with u
+// rounded to nearest (random/src/lcg32.cpp:231-240 and the '< p_add' of its callers).  The
+// scaling by 2^-32 is exact and round-to-nearest conversion is monotone in u, so the accepted
+// u are exactly the prefix [0, thr) with thr = accept_threshold(p_add): one integer compare.
+__device__ __forceinline__ bool lcg_accept(uint32_t u, uint32_t thr)
 {
-    return __fmul_rn(__uint2float_rn(u), kTwoPowMinus32) < p_add;
+    return u < thr;
+}
+
+// Smallest u with (float)u >= p_add * 2^32, by bisection with the same round-to-nearest
+// conversion (host code; p_add in [0, 1], so the answer is below 2^32).
+inline uint32_t accept_threshold(float p_add)
+{
+    const float q = p_add * 4294967296.0f;  // exact: power-of-two scaling
+    uint64_t lo = 0, hi = 1ull << 32;
+    while (lo < hi) {
+        const uint64_t mid = (lo + hi) >> 1;
+        if (static_cast<float>(static_cast<uint32_t>(mid)) >= q)
+            hi = mid;
+        else
+            lo = mid + 1;
+    }
+    return static_cast<uint32_t>(lo);
 }
 
 // ---- drand48: X' = 0x5DEECE66D X + 0xB mod 2^48 (POSIX), used by LCG32_State::Init and the

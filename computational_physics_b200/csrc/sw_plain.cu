@@ -65,11 +65,11 @@ template <int W>
 __global__ void __launch_bounds__(kAssignThreads, 4) k_assign(const Geo g, const uint8_t *__restrict__ spins,
                                                  uint32_t *__restrict__ labels, uint32_t *__restrict__ rng_state,
                                                  uint8_t *__restrict__ rng_sel, uint32_t *__restrict__ rng_iter,
-                                                 const float p_add, uint32_t *__restrict__ edge,
+                                                 const uint32_t thr, uint32_t *__restrict__ edge,
                                                  uint8_t *__restrict__ dbg_bonds, uint32_t *__restrict__ dbg_assign)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    assign_block<W>(g, blockIdx.x, blockIdx.y, spins, labels, rng_state, rng_sel, rng_iter, p_add, edge, dbg_bonds,
+    assign_block<W>(g, blockIdx.x, blockIdx.y, spins, labels, rng_state, rng_sel, rng_iter, thr, edge, dbg_bonds,
                     dbg_assign, smem);
 }
 
@@ -255,7 +255,8 @@ int launch_assign_w(swb_lattice *h, float p_add, uint8_t *dbg_bonds, uint32_t *d
     // Whole warps: the draws use full-warp shuffles and ballots; surplus lanes have no tile.
     const dim3 grid(g.nbx, g.nby), block((g.TBX * g.TBY * W + 31) / 32 * 32);
     k_assign<W><<<grid, block, h->smem_assign, h->stream>>>(g, h->spins, h->labels, h->rng_state, h->rng_sel,
-                                                            h->rng_iter, p_add, h->edge, dbg_bonds, dbg_assign);
+                                                            h->rng_iter, accept_threshold(p_add), h->edge, dbg_bonds,
+                                                            dbg_assign);
     SWB_LAUNCHED();
     return SWB_OK;
 }
@@ -340,6 +341,8 @@ uint64_t swb_kernel_launches(void) { return g_launches.load(); }
 
 float swb_p_add(float temperature) { return 1.0f - static_cast<float>(std::exp(-2.0f / temperature)); }
 
+uint32_t swb_accept_threshold(float p_add) { return accept_threshold(p_add); }
+
 int swb_create(swb_lattice **out, uint32_t L0, uint32_t L1, uint32_t tile_x, uint32_t tile_y, uint32_t lcg_width,
                uint32_t seed_base, int device)
 {
@@ -348,8 +351,8 @@ int swb_create(swb_lattice **out, uint32_t L0, uint32_t L1, uint32_t tile_x, uin
     *out = nullptr;
     if (L0 == 0 || L1 == 0 || (L0 % 2) || (L1 % 2))
         return fail(SWB_ERR_ARGUMENT, "SwendsenWang_2D implementation requires evenly sized lattice (%u x %u)", L0, L1);
-    if ((uint64_t)L0 * L1 > 0xFFFFFFFFull)
-        return fail(SWB_ERR_ARGUMENT, "lattice of %u x %u sites exceeds 32-bit labels", L0, L1);
+    if ((uint64_t)L0 * L1 > 0x7FFFFFFFull)
+        return fail(SWB_ERR_ARGUMENT, "lattice of %u x %u sites exceeds 2^31 - 1 labels", L0, L1);
     if (!(tile_x == 8 || tile_x == 16 || tile_x == 32) || tile_y < 2 || tile_y > 32)
         return fail(SWB_ERR_ARGUMENT, "unsupported tile %u x %u (tile_x in {8,16,32}, 2 <= tile_y <= 32)", tile_x, tile_y);
     if (!valid_width(lcg_width))

@@ -51,7 +51,8 @@ uint64_t swb_kernel_launches(void);
 /* Creates an L0 x L1 periodic lattice on CUDA device `device` with tiles tile_x x tile_y
  * and lcg32 streams of `lcg_width` lanes seeded seed_base + tile id.  Replaces
  * SwendsenWang_2D::Initialize (ising/src/swendsen_wang.cpp:148-199): extents must be
- * even (:154-155); labels fit uint32 (swendsen_wang.hpp:29-30).  tile_x in {8, 16, 32},
+ * even (:154-155); at most 2^31 - 1 sites (labels are uint32, swendsen_wang.hpp:29-30, with
+ * the top bit used internally).  tile_x in {8, 16, 32},
  * 2 <= tile_y <= 32, lcg_width in {8, 16, 32}.  Spins start all 0. */
 int swb_create(swb_lattice **out, uint32_t L0, uint32_t L1, uint32_t tile_x, uint32_t tile_y,
                uint32_t lcg_width, uint32_t seed_base, int device);
@@ -76,6 +77,10 @@ int swb_cold_start(swb_lattice *h, uint8_t value);
 
 /* p_add = 1 - exp(-2/T) in float, as ising/src/swendsen_wang.cpp:207. */
 float swb_p_add(float temperature);
+
+/* The integer form of the bond test: a draw u is accepted iff u < swb_accept_threshold(p_add),
+ * which equals the reference's (float)u * 2^-32 < p_add (random/src/lcg32.cpp:231-240). */
+uint32_t swb_accept_threshold(float p_add);
 
 /* n_sweeps sweeps at `temperature`: SwendsenWang_2D::Update (ising/src/swendsen_wang.cpp:201-219)
  * -- bond activation + tile labelling, boundary merge, label resolution, cluster flip.  If
@@ -119,7 +124,9 @@ int swb_get_rng(swb_lattice *h, uint32_t *state, uint32_t *a, uint32_t *c, uint3
 int swb_set_rng(swb_lattice *h, const uint32_t *state, const uint32_t *a, const uint32_t *c,
                 const uint32_t *iteration);
 
-/* Device pointers of the spin and label arrays (for zero-copy interop; valid until destroy). */
+/* Device pointers of the spin and label arrays (for zero-copy interop; valid until destroy).
+ * Between sweeps the label array holds the engine's internal encoding; resolved labels (the
+ * minimum site index of each cluster) are there after swb_sweep_recorded. */
 int swb_device_buffers(swb_lattice *h, void **spins, void **labels);
 
 /* Number of kernel launches one plain sweep issues on this handle. */

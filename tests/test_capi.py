@@ -56,3 +56,23 @@ def test_pure_host_entry_points_without_gpu():
     assert lib.swb_create(ctypes.byref(h), 16, 16, 12, 8, 16, 1, 0) == 1          # tile width
     assert lib.swb_create(ctypes.byref(h), 16, 16, 16, 8, 12, 1, 0) == 1          # lcg width
     assert not h.value
+
+
+def test_accept_threshold_is_the_reference_float_test():
+    """u < swb_accept_threshold(p) must equal (float)u * 2^-32 < p for every u; checked at the
+    threshold's neighbourhood and on random draws for many p, with numpy's round-to-nearest."""
+    import numpy as np
+    import computational_physics_b200 as cp
+    lib = cp.lib()
+    rng = np.random.default_rng(7)
+    scale = np.float32(2.0 ** -32)
+    ps = np.concatenate([np.float32([0.0, 1.0, 0.5, 0.5857864618301392, 1e-7, 0.9999999]),
+                         rng.random(200).astype(np.float32),
+                         np.array([cp.p_add(float(t)) for t in np.linspace(0.3, 6, 100)], np.float32)])
+    for p in ps:
+        thr = int(lib.swb_accept_threshold(float(p)))
+        us = np.concatenate([rng.integers(0, 2 ** 32, 2000, dtype=np.uint64),
+                             np.arange(max(thr - 300, 0), min(thr + 300, 2 ** 32), dtype=np.uint64)]).astype(np.uint32)
+        want = (us.astype(np.float32) * scale) < np.float32(p)
+        got = us.astype(np.uint64) < thr
+        assert np.array_equal(want, got), float(p)
