@@ -100,23 +100,23 @@ __device__ __forceinline__ uint32_t label_global(const Geo &g, uint32_t bxi, uin
 }
 
 struct AssignSmem {
-    uint32_t parent, accM, accX, accY, edge, bond, sp, total, pitch;
+    uint32_t parent, accM, accX, accY, edge, bond, sp, plab, total, pitch;
 };
 
 __host__ __device__ inline AssignSmem assign_smem(const Geo &g)
 {
     AssignSmem s{};
     const uint32_t ns = g.BX * g.BY, ntb = g.TBX * g.TBY;
-    s.pitch = g.BX + 4;
+    s.pitch = g.BX + 16;  // rows 16-byte aligned for cp.async
     s.parent = 0;
     s.accM = s.parent + ns * 4;
     s.accX = s.accM + ntb * 8;
     s.accY = s.accX + ntb * g.TY * 4;
     s.edge = s.accY + ntb * g.TY * 4;
     s.bond = s.edge + kEdgeWords * 4;
-    s.sp = s.bond + ns;
-    s.total = s.sp + (g.BY + 1) * s.pitch;
-    s.total = (s.total + 15) & ~15u;
+    s.sp = (s.bond + ns + 15) & ~15u;
+    s.plab = (s.sp + (g.BY + 1) * s.pitch + 15) & ~15u;  // uint16 provisional labels (row path)
+    s.total = (s.plab + 2 * ns + 15) & ~15u;
     return s;
 }
 
@@ -168,6 +168,7 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
         const uint32_t jjmax = byv > tby * g.TY ? min(g.TY, byv - tby * g.TY) : 0;
         for (uint32_t w = 0; w < NW; ++w) {
             const uint32_t xl = (w << 5) + lane;
+            parent[yl * BX + xl] = yl * BX + xl;
             bool xb = false, yb = false;
             if (xl < bxv && yl < byv) {
                 const uint32_t tbx = xl >> txs, tb = tby * g.TBX + tbx;
@@ -198,47 +199,67 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
     }
     __syncthreads();
 
-    // parent = first site of the x-bonded run
-    for (uint32_t yl = warp; yl < BY; yl += nwarps) {
-        uint32_t carry = 0, carry_on = 0;
-        for (uint32_t w = 0; w < NW; ++w) {
-            const uint32_t X = Xw[yl * NW + w];
+    // Scanline labelling.  Work item = (32-column strip, band of rows); a warp walks its band
+    // top-down with each lane holding the provisional label of the site above.  A run (x-bonded
+    // sites of the strip row, found from the gap mask) takes the minimum of the labels reaching
+    // it through y-bonds -- a segmented min over the run by five shfl_up steps -- or, with none,
+    // its own first site as a new label.  Two different labels meeting in a run are united in
+    // the shared union-find (toward the minimum).  Seams between strips and bands are united
+    // afterwards, then every site resolves its provisional label.
+    uint16_t *plab = reinterpret_cast<uint16_t *>(smem + L.plab);
+    const uint32_t nb = max(1u, nwarps / NW);                // bands
+    const uint32_t rb = (BY + nb - 1) / nb;                  // rows per band
+    for (uint32_t task = warp; task < NW * nb; task += nwarps) {
+        const uint32_t sx = task % NW, band = task / NW;
+        const uint32_t ya = band * rb, yb = min(BY, ya + rb);
+        uint32_t above = 0xFFFFFFFFu;
+        for (uint32_t yl = ya; yl < yb; ++yl) {
+            const uint32_t X = Xw[yl * NW + sx];
+            const uint32_t Yup = yl > ya ? Yw[(yl - 1) * NW + sx] : 0u;
             const uint32_t gaps = ~X & ((1u << lane) - 1u);
-            const uint32_t start = gaps ? (w << 5) + 32 - __clz(gaps) : (carry_on ? carry : (w << 5));
-            parent[yl * BX + (w << 5) + lane] = yl * BX + start;
-            carry = __shfl_sync(0xffffffffu, start, 31);
-            carry_on = X >> 31;
+            const uint32_t rs = gaps ? 32 - __clz(gaps) : 0;            // run start (lane)
+            const uint32_t re = __ffs(~X & (0xFFFFFFFFu << lane)) - 1;   // run end (lane); X bit 31 never ends a strip run
+            const bool up = (Yup >> lane) & 1u;
+            uint32_t c = up ? above : 0xFFFFFFFFu;
+#pragma unroll
+            for (uint32_t d = 1; d < 32; d <<= 1) {
+                const uint32_t v = __shfl_up_sync(0xffffffffu, c, d);
+                if (lane >= rs + d)
+                    c = min(c, v);
+            }
+            const uint32_t m = __shfl_sync(0xffffffffu, c, re == 0xFFFFFFFFu ? 31 : re);
+            const uint32_t lab = m != 0xFFFFFFFFu ? m : yl * BX + (sx << 5) + rs;
+            if (up && above != lab)
+                uf_union(parent, above, lab);
+            plab[yl * BX + (sx << 5) + lane] = (uint16_t)lab;
+            above = lab;
         }
     }
     __syncthreads();
 
-    // vertical bonds, skipping those whose left neighbour already joins the same two runs
-    for (uint32_t yl = warp; yl + 1 < BY; yl += nwarps) {
-        uint32_t prev = 0;
-        for (uint32_t w = 0; w < NW; ++w) {
-            const uint32_t Y = Yw[yl * NW + w];
-            const uint32_t X = Xw[yl * NW + w], Xb = Xw[(yl + 1) * NW + w];
-            const uint32_t T = Y & X & Xb;
-            const uint32_t U = Y & ~((T << 1) | prev);
-            prev = T >> 31;
-            if ((U >> lane) & 1u) {
-                const uint32_t l = yl * BX + (w << 5) + lane;
-                uf_union(parent, l, l + BX);
-            }
+    // Seams: y-bonds from the last row of a band into the next band (skipping those whose left
+    // neighbour already joins the same runs), and x-bonds from a strip's last column into the
+    // next strip.
+    for (uint32_t task = warp; task < (nb - 1) * NW; task += nwarps) {
+        const uint32_t sx = task % NW, yl = (task / NW + 1) * rb - 1;
+        if (yl + 1 >= BY)
+            continue;
+        const uint32_t Y = Yw[yl * NW + sx];
+        const uint32_t X = Xw[yl * NW + sx], Xb = Xw[(yl + 1) * NW + sx];
+        const uint32_t prevT = sx ? ((Yw[yl * NW + sx - 1] & Xw[yl * NW + sx - 1] & Xw[(yl + 1) * NW + sx - 1]) >> 31) : 0u;
+        const uint32_t U = Y & ~(((Y & X & Xb) << 1) | prevT);
+        if ((U >> lane) & 1u) {
+            const uint32_t l = yl * BX + (sx << 5) + lane;
+            uf_union(parent, plab[l], plab[l + BX]);
         }
     }
-    __syncthreads();
-
-    // Roots of the runs: every run's first site follows its chain once and points straight at
-    // the block root; afterwards any site's root is parent[parent[site]] (its run start's).
-    for (uint32_t yl = warp; yl < BY; yl += nwarps)
-        for (uint32_t w = 0; w < NW; ++w) {
-            const uint32_t left = lane ? (Xw[yl * NW + w] >> (lane - 1)) & 1u : (w ? Xw[yl * NW + w - 1] >> 31 : 0u);
-            if (!left) {
-                const uint32_t l = yl * BX + (w << 5) + lane;
-                parent[l] = uf_find(parent, l);
-            }
+    for (uint32_t i = tid; i < BY * (NW - 1); i += blockDim.x) {
+        const uint32_t yl = i / (NW - 1), sx = i - yl * (NW - 1);
+        if (Xw[yl * NW + sx] >> 31) {
+            const uint32_t l = yl * BX + (sx << 5) + 31;
+            uf_union(parent, plab[l], plab[l + 1]);
         }
+    }
     __syncthreads();
 
     // Labels: a block root stores its global site index (the merge links these), every other
@@ -249,7 +270,7 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
             const uint32_t xl = (w << 5) + lane;
             if (xl < bxv) {
                 const uint32_t l = yl * BX + xl;
-                const uint32_t r = parent[parent[l]];
+                const uint32_t r = uf_find_halve(parent, plab[l]);
                 row[xl] = r == l ? (y0 + yl) * g.L0 + x0 + xl : (kLocalFlag | r);
             }
         }
@@ -286,27 +307,37 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
     if (tid < kEdgeWords)
         edge_s[tid] = 0;
 
-    // ---- 1. spins of the block and its halo (column x0+bxv and row y0+byv, periodic)
+    // ---- 1. spins of the block and its halo (column x0+bxv and row y0+byv, periodic).  Rows
+    // go global -> shared by cp.async, in flight while the lcg32 draws below run; the strided
+    // halo column is one byte per thread, held in a register until then.
+    const uint32_t hx = (x0 + bxv) % g.L0;
+    uint8_t halo = 0;
     {
         const uint32_t warp = tid >> 5, lane32 = tid & 31, nwarps = nthr >> 5;
-        const uint32_t hx = (x0 + bxv) % g.L0, hy = (y0 + byv) % g.L1;
-        const bool words = (g.L0 % 4) == 0;
+        const uint32_t hy = (y0 + byv) % g.L1;
+        const uint32_t vec = (g.L0 % 16 == 0 && BX % 16 == 0) ? 16 : (g.L0 % 4 == 0 ? 4 : 1);
         for (uint32_t yl = warp; yl <= byv; yl += nwarps) {
             const uint32_t gy = yl < byv ? y0 + yl : hy;
             const uint8_t *row = spins + (size_t)gy * g.L0 + x0;
             uint8_t *dst = sp + yl * pitch;
-            if (words) {
-                for (uint32_t w = lane32; w * 4 < bxv; w += 32)
-                    *reinterpret_cast<uint32_t *>(dst + 4 * w) = __ldg(reinterpret_cast<const uint32_t *>(row) + w);
+            if (vec == 16) {
+                for (uint32_t v = lane32; v * 16 < bxv; v += 32)
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(
+                                     (uint32_t)__cvta_generic_to_shared(dst + 16 * v)),
+                                 "l"(row + 16 * v));
+            } else if (vec == 4) {
+                for (uint32_t v = lane32; v * 4 < bxv; v += 32)
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(
+                                     (uint32_t)__cvta_generic_to_shared(dst + 4 * v)),
+                                 "l"(row + 4 * v));
             } else {
                 for (uint32_t x = lane32; x < bxv; x += 32)
                     dst[x] = __ldg(row + x);
             }
         }
-        for (uint32_t yl = tid; yl < byv; yl += nthr)
-            sp[yl * pitch + bxv] = __ldg(spins + (size_t)(y0 + yl) * g.L0 + hx);
+        if (tid < byv)
+            halo = __ldg(spins + (size_t)(y0 + tid) * g.L0 + hx);
     }
-    __syncthreads();
 
     // ---- 2. lcg32 draws of this sweep, one W-lane segment per tile
     {
@@ -384,6 +415,9 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
         if (lane == 0 && tb < ntb)
             accM[tb] = mbits;
     }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    if (tid < byv)
+        sp[tid * pitch + bxv] = halo;
     __syncthreads();
 
     if (dbg_assign == nullptr && (BX & 31u) == 0 && (BX & (BX - 1)) == 0) {

@@ -98,12 +98,29 @@ __device__ __forceinline__ uint32_t uf_find(const volatile uint32_t *p, uint32_t
     return x;
 }
 
-__device__ __forceinline__ void uf_union(uint32_t *p, uint32_t a, uint32_t b)
+// Find that halves the path on the way (x's parent becomes its grandparent).  The update is
+// an atomicMin, which only moves a pointer further toward the root, so it is safe while other
+// threads unite; it keeps the trees that concurrent unions build shallow.
+__device__ __forceinline__ uint32_t uf_find_halve(uint32_t *p, uint32_t x)
 {
     const volatile uint32_t *vp = p;
+    uint32_t y = vp[x];
+    while (y != x) {
+        const uint32_t z = vp[y];
+        if (z == y)
+            return y;
+        atomicMin(p + x, z);
+        x = z;
+        y = vp[x];
+    }
+    return x;
+}
+
+__device__ __forceinline__ void uf_union(uint32_t *p, uint32_t a, uint32_t b)
+{
     while (true) {
-        a = uf_find(vp, a);
-        b = uf_find(vp, b);
+        a = uf_find_halve(p, a);
+        b = uf_find_halve(p, b);
         if (a == b)
             return;
         if (a > b) {
