@@ -102,8 +102,8 @@ __global__ void __launch_bounds__(kBatchThreads, 4) kb_assign(BatchLat *lats, co
             continue;
         const Geo g = L->g;
         const uint32_t blk = item - blk_prefix[k];
-        assign_block<W>(g, blk % g.nbx, blk / g.nbx, L->spins, L->labels, L->rng_state, L->rng_sel, L->rng_iter,
-                        L->thr, L->edge, nullptr, nullptr, smem);
+        assign_block_any<W>(g, blk % g.nbx, blk / g.nbx, L->spins, L->labels, L->rng_state, L->rng_sel, L->rng_iter,
+                            L->thr, L->edge, smem);
         __syncthreads();
     }
 }

@@ -142,11 +142,13 @@ struct LatView {
 // bonds need no union; a vertical bond is united only when the bond to its left does not
 // already join the same two runs.  The result equals the generic path's: the minimum site
 // index of each block-local component.
+template <int TXc, int TYc>
 __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uint32_t bxi, const uint32_t byi,
                                                          uint32_t *__restrict__ labels, uint32_t *__restrict__ edge,
                                                          unsigned char *smem)
 {
     const AssignSmem L = assign_smem(g);
+    const uint32_t TX = TXc ? TXc : g.TX, TY = TYc ? TYc : g.TY;  // compile-time for the common tiles
     uint32_t *parent = reinterpret_cast<uint32_t *>(smem + L.parent);
     const uint64_t *accM = reinterpret_cast<const uint64_t *>(smem + L.accM);
     const uint32_t *accX = reinterpret_cast<const uint32_t *>(smem + L.accX);
@@ -160,12 +162,12 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
     const uint32_t x0 = bxi * BX, y0 = byi * BY;
     const uint32_t bxv = min(BX, g.L0 - x0), byv = min(BY, g.L1 - y0);
     const uint32_t pitch = L.pitch;
-    const uint32_t txs = 31 - __clz(g.TX);  // TX is 8, 16 or 32
+    const uint32_t txs = TXc ? (TXc == 8 ? 3 : TXc == 16 ? 4 : 5) : 31 - __clz(TX);  // TX is 8, 16 or 32
 
     // bond words; edge bonds go to edge_s (right edge: one bit per row, bottom: the row's words)
     for (uint32_t yl = warp; yl < BY; yl += nwarps) {
-        const uint32_t tby = yl / g.TY, jj = yl - tby * g.TY;
-        const uint32_t jjmax = byv > tby * g.TY ? min(g.TY, byv - tby * g.TY) : 0;
+        const uint32_t tby = yl / TY, jj = yl - tby * TY;
+        const uint32_t jjmax = byv > tby * TY ? min(TY, byv - tby * TY) : 0;
         for (uint32_t w = 0; w < NW; ++w) {
             const uint32_t xl = (w << 5) + lane;
             parent[yl * BX + xl] = yl * BX + xl;
@@ -173,10 +175,10 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
             if (xl < bxv && yl < byv) {
                 const uint32_t tbx = xl >> txs, tb = tby * g.TBX + tbx;
                 const uint32_t ii = xl - (tbx << txs);
-                const uint32_t iimax = min(g.TX, bxv - (tbx << txs));
+                const uint32_t iimax = min(TX, bxv - (tbx << txs));
                 const uint8_t s = sp[yl * pitch + xl];
-                const uint32_t xa = (ii + 1 < iimax) ? (accX[tb * g.TY + jj] >> ii) : (uint32_t)(accM[tb] >> (g.TX + jj));
-                const uint32_t ya = (jj + 1 < jjmax) ? (accY[tb * g.TY + jj] >> ii) : (uint32_t)(accM[tb] >> ii);
+                const uint32_t xa = (ii + 1 < iimax) ? (accX[tb * TY + jj] >> ii) : (uint32_t)(accM[tb] >> (TX + jj));
+                const uint32_t ya = (jj + 1 < jjmax) ? (accY[tb * TY + jj] >> ii) : (uint32_t)(accM[tb] >> ii);
                 xb = (xa & 1u) && s == sp[yl * pitch + xl + 1];
                 yb = (ya & 1u) && s == sp[(yl + 1) * pitch + xl];
             }
@@ -281,7 +283,7 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
 
 // Block (bxi, byi) of a lattice: lcg32 draws, bonds, union-find in shared memory.  Runs on
 // all threads of the CTA (at least TBX * TBY * W of them); smem holds assign_smem(g).total bytes.
-template <int W>
+template <int W, int TXc = 0, int TYc = 0>
 __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, const uint32_t byi,
                                              const uint8_t *__restrict__ spins, uint32_t *__restrict__ labels,
                                              uint32_t *__restrict__ rng_state, uint8_t *__restrict__ rng_sel,
@@ -290,6 +292,7 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
                                              uint32_t *__restrict__ dbg_assign, unsigned char *smem)
 {
     const AssignSmem L = assign_smem(g);
+    const uint32_t TX = TXc ? TXc : g.TX, TY = TYc ? TYc : g.TY;  // compile-time for the common tiles
     uint32_t *parent = reinterpret_cast<uint32_t *>(smem + L.parent);
     uint64_t *accM = reinterpret_cast<uint64_t *>(smem + L.accM);
     uint32_t *accX = reinterpret_cast<uint32_t *>(smem + L.accX);
@@ -345,7 +348,7 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
         const uint32_t tgx = bxi * g.TBX + tb % g.TBX, tgy = byi * g.TBY + tb / g.TBX;
         const bool on = tb < ntb && tgx < g.n0 && tgy < g.n1;
         const uint32_t tile = tgy * g.n0 + tgx;
-        const uint32_t jjmax = on ? min(g.TY, g.L1 - tgy * g.TY) : 0;
+        const uint32_t jjmax = on ? min(TY, g.L1 - tgy * TY) : 0;
         uint32_t st = 0, sel = 0, it = 0;
         if (on) {
             st = rng_state[(size_t)tile * W + lane];
@@ -354,7 +357,7 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
         }
         uint32_t a = lcg_param_a(sel), c = lcg_param_c(sel);
         uint32_t to_rot = kShuffleDistance - it % kShuffleDistance;  // updates until the next rotation
-        const uint32_t Ur = (g.TX + W - 1) / W, Um = (g.TX + g.TY + W - 1) / W;
+        const uint32_t Ur = (TX + W - 1) / W, Um = (TX + TY + W - 1) / W;
         const uint32_t nrow = on ? 2 * jjmax - 1 : 0;
         const uint32_t seg_shift = ((tid & 31) / W) * W;
         const uint32_t seg_mask = (W == 32) ? 0xffffffffu : ((1u << (W & 31)) - 1u);
@@ -384,26 +387,26 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
         // Row requests: tile_x numbers each, x-bond rows then y-bond rows; element k is lane
         // k % W after update k / W + 1 of the request.  The ballot gives every lane the whole
         // word; one lane stores it.
-        for (uint32_t req = 0; req < 2 * g.TY - 1; ++req) {
+        for (uint32_t req = 0; req < 2 * TY - 1; ++req) {
             const bool upd = req < nrow;
             uint32_t word = 0;
             for (uint32_t sub = 0; sub < Ur; ++sub) {
                 advance(upd);
-                const bool bit = upd && sub * W + lane < g.TX && lcg_accept(st, thr);
+                const bool bit = upd && sub * W + lane < TX && lcg_accept(st, thr);
                 word |= ((__ballot_sync(0xffffffffu, bit) >> seg_shift) & seg_mask) << (sub * W);
             }
             if (upd && lane == (req & (W - 1))) {
                 if (req < jjmax)
-                    accX[tb * g.TY + req] = word;
+                    accX[tb * TY + req] = word;
                 else
-                    accY[tb * g.TY + req - jjmax] = word;
+                    accY[tb * TY + req - jjmax] = word;
             }
         }
         // The merge request: tile_x + tile_y numbers, [0, tile_x) bottom edge, then right edge.
         uint64_t mbits = 0;
         for (uint32_t sub = 0; sub < Um; ++sub) {
             advance(on);
-            const bool bit = on && sub * W + lane < g.TX + g.TY && lcg_accept(st, thr);
+            const bool bit = on && sub * W + lane < TX + TY && lcg_accept(st, thr);
             mbits |= (uint64_t)((__ballot_sync(0xffffffffu, bit) >> seg_shift) & seg_mask) << (sub * W);
         }
         if (on) {
@@ -421,7 +424,7 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
     __syncthreads();
 
     if (dbg_assign == nullptr && (BX & 31u) == 0 && (BX & (BX - 1)) == 0) {
-        assign_block_labels_rows(g, bxi, byi, labels, edge, smem);
+        assign_block_labels_rows<TXc, TYc>(g, bxi, byi, labels, edge, smem);
         return;
     }
 
@@ -431,12 +434,12 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
         const uint32_t xl = l % BX, yl = l / BX;
         uint8_t b = 0;
         if (xl < bxv && yl < byv) {
-            const uint32_t tbx = xl / g.TX, tby = yl / g.TY, tb = tby * g.TBX + tbx;
-            const uint32_t ii = xl - tbx * g.TX, jj = yl - tby * g.TY;
-            const uint32_t iimax = min(g.TX, bxv - tbx * g.TX), jjmax = min(g.TY, byv - tby * g.TY);
+            const uint32_t tbx = xl / TX, tby = yl / TY, tb = tby * g.TBX + tbx;
+            const uint32_t ii = xl - tbx * TX, jj = yl - tby * TY;
+            const uint32_t iimax = min(TX, bxv - tbx * TX), jjmax = min(TY, byv - tby * TY);
             const uint8_t s = sp[yl * pitch + xl];
-            const uint32_t xa = (ii + 1 < iimax) ? (accX[tb * g.TY + jj] >> ii) : (uint32_t)(accM[tb] >> (g.TX + jj));
-            const uint32_t ya = (jj + 1 < jjmax) ? (accY[tb * g.TY + jj] >> ii) : (uint32_t)(accM[tb] >> ii);
+            const uint32_t xa = (ii + 1 < iimax) ? (accX[tb * TY + jj] >> ii) : (uint32_t)(accM[tb] >> (TX + jj));
+            const uint32_t ya = (jj + 1 < jjmax) ? (accY[tb * TY + jj] >> ii) : (uint32_t)(accM[tb] >> ii);
             b = (uint8_t)(((xa & 1u) && s == sp[yl * pitch + xl + 1]) | (((ya & 1u) && s == sp[(yl + 1) * pitch + xl]) << 1));
         }
         bond[l] = b;
@@ -450,9 +453,9 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
         if (!b)
             continue;
         const uint32_t xl = l % BX, yl = l / BX;
-        const uint32_t tbx = xl / g.TX, tby = yl / g.TY;
-        const uint32_t ii = xl - tbx * g.TX, jj = yl - tby * g.TY;
-        const uint32_t iimax = min(g.TX, bxv - tbx * g.TX), jjmax = min(g.TY, byv - tby * g.TY);
+        const uint32_t tbx = xl / TX, tby = yl / TY;
+        const uint32_t ii = xl - tbx * TX, jj = yl - tby * TY;
+        const uint32_t iimax = min(TX, bxv - tbx * TX), jjmax = min(TY, byv - tby * TY);
         if ((b & 1) && ii + 1 < iimax)
             uf_union(parent, l, l + 1);
         if ((b & 2) && jj + 1 < jjmax)
@@ -478,9 +481,9 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
         if (!b)
             continue;
         const uint32_t xl = l % BX, yl = l / BX;
-        const uint32_t tbx = xl / g.TX, tby = yl / g.TY;
-        const uint32_t ii = xl - tbx * g.TX, jj = yl - tby * g.TY;
-        const uint32_t iimax = min(g.TX, bxv - tbx * g.TX), jjmax = min(g.TY, byv - tby * g.TY);
+        const uint32_t tbx = xl / TX, tby = yl / TY;
+        const uint32_t ii = xl - tbx * TX, jj = yl - tby * TY;
+        const uint32_t iimax = min(TX, bxv - tbx * TX), jjmax = min(TY, byv - tby * TY);
         if ((b & 1) && ii + 1 == iimax) {
             if (xl + 1 < bxv)
                 uf_union(parent, l, l + 1);
@@ -507,6 +510,34 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
     }
     if (tid < kEdgeWords)
         edge[((size_t)byi * g.nbx + bxi) * kEdgeWords + tid] = edge_s[tid];
+}
+
+// assign_block with the tile shape as compile-time constants for the common shapes (lcg width
+// 16), the runtime form otherwise.
+template <int W>
+__device__ __forceinline__ void assign_block_any(const Geo &g, const uint32_t bxi, const uint32_t byi,
+                                                 const uint8_t *__restrict__ spins, uint32_t *__restrict__ labels,
+                                                 uint32_t *__restrict__ rng_state, uint8_t *__restrict__ rng_sel,
+                                                 uint32_t *__restrict__ rng_iter, const uint32_t thr,
+                                                 uint32_t *__restrict__ edge, unsigned char *smem)
+{
+#define SWB_TILE(tx, ty)                                                                                              \
+    if (g.TX == tx && g.TY == ty) {                                                                                   \
+        assign_block<W, tx, ty>(g, bxi, byi, spins, labels, rng_state, rng_sel, rng_iter, thr, edge, nullptr, nullptr, \
+                                smem);                                                                                \
+        return;                                                                                                       \
+    }
+    if (W == 16) {
+        SWB_TILE(16, 8)
+        SWB_TILE(8, 8)
+        SWB_TILE(32, 4)
+        SWB_TILE(16, 16)
+        SWB_TILE(8, 16)
+        SWB_TILE(32, 8)
+        SWB_TILE(16, 4)
+    }
+#undef SWB_TILE
+    assign_block<W>(g, bxi, byi, spins, labels, rng_state, rng_sel, rng_iter, thr, edge, nullptr, nullptr, smem);
 }
 
 // Unions across the right and bottom edge (periodic) of block blk: thread t < BY takes row
@@ -566,6 +597,51 @@ __device__ __forceinline__ void flip_block(const Geo &g, const uint32_t bxi, con
     const uint32_t x0 = bxi * BX, y0 = byi * g.BY;
     const uint32_t bxv = min(BX, L0 - x0), byv = min(g.BY, g.L1 - y0);
     const uint32_t base = y0 * L0 + x0;
+    const uint32_t nq = (bxv >> 2) * byv, qrow = bxv >> 2;
+    if ((L0 & 3u) == 0 && nq <= 2 * blockDim.x) {
+        // Every thread holds at most two quads (4 labels + 4 spins each) in registers: one
+        // round trip for the loads, the roots' chains, then the flips.
+        uint4 lab[2];
+        uint32_t spn[2], sidx[2], lidx[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const uint32_t qi = tid + k * blockDim.x;
+            if (qi < nq) {
+                const uint32_t yl = qi / qrow, xq = qi - yl * qrow;
+                sidx[k] = base + yl * L0 + 4 * xq;
+                lidx[k] = yl * BX + 4 * xq;
+                lab[k] = *reinterpret_cast<const uint4 *>(labels + sidx[k]);
+                spn[k] = reinterpret_cast<const uint32_t *>(spins)[sidx[k] >> 2];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            if (tid + k * blockDim.x < nq) {
+                const uint32_t v[4] = {lab[k].x, lab[k].y, lab[k].z, lab[k].w};
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (!(v[j] & kLocalFlag))
+                        res[lidx[k] + j] = guf_find(labels, sidx[k] + j, fault);
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            if (tid + k * blockDim.x < nq) {
+                const uint32_t v[4] = {lab[k].x, lab[k].y, lab[k].z, lab[k].w};
+                uint32_t r[4], flip = 0;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    r[j] = res[(v[j] & kLocalFlag) ? (v[j] & kLocalMask) : lidx[k] + j];
+                    flip |= (r[j] & 1u) << (8 * j);
+                }
+                reinterpret_cast<uint32_t *>(spins)[sidx[k] >> 2] = spn[k] ^ flip;
+                if (kWriteLabels)
+                    *reinterpret_cast<uint4 *>(labels + sidx[k]) = make_uint4(r[0], r[1], r[2], r[3]);
+            }
+        }
+        return;
+    }
     for (uint32_t yl = warp; yl < byv; yl += nwarps)
         for (uint32_t xl = lane; xl < bxv; xl += 32) {
             const uint32_t site = base + yl * L0 + xl;

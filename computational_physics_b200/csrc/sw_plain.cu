@@ -61,7 +61,9 @@ int fail(int code, const char *fmt, ...)
 
 constexpr uint32_t kAssignThreads = 512;  // at most this many lcg lanes per block
 
-template <int W>
+// kDebug adds the stage dumps (bond bytes and tile-local labels) of a recorded sweep.  TXc, TYc
+// make the tile shape a compile-time constant for the common shapes (0 = runtime).
+template <int W, int TXc, int TYc, bool kDebug>
 __global__ void __launch_bounds__(kAssignThreads, 4) k_assign(const Geo g, const uint8_t *__restrict__ spins,
                                                  uint32_t *__restrict__ labels, uint32_t *__restrict__ rng_state,
                                                  uint8_t *__restrict__ rng_sel, uint32_t *__restrict__ rng_iter,
@@ -69,8 +71,8 @@ __global__ void __launch_bounds__(kAssignThreads, 4) k_assign(const Geo g, const
                                                  uint8_t *__restrict__ dbg_bonds, uint32_t *__restrict__ dbg_assign)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    assign_block<W>(g, blockIdx.x, blockIdx.y, spins, labels, rng_state, rng_sel, rng_iter, thr, edge, dbg_bonds,
-                    dbg_assign, smem);
+    assign_block<W, TXc, TYc>(g, blockIdx.x, blockIdx.y, spins, labels, rng_state, rng_sel, rng_iter, thr, edge,
+                              kDebug ? dbg_bonds : nullptr, kDebug ? dbg_assign : nullptr, smem);
 }
 
 __global__ void __launch_bounds__(256) k_merge(const Geo g, const uint32_t *__restrict__ edge, uint32_t *labels,
@@ -248,17 +250,35 @@ int set_device(const swb_lattice *h)
     return SWB_OK;
 }
 
-template <int W>
-int launch_assign_w(swb_lattice *h, float p_add, uint8_t *dbg_bonds, uint32_t *dbg_assign)
+template <int W, int TXc, int TYc, bool kDebug>
+int launch_assign_k(swb_lattice *h, float p_add, uint8_t *dbg_bonds, uint32_t *dbg_assign)
 {
     const Geo &g = h->g;
     // Whole warps: the draws use full-warp shuffles and ballots; surplus lanes have no tile.
     const dim3 grid(g.nbx, g.nby), block((g.TBX * g.TBY * W + 31) / 32 * 32);
-    k_assign<W><<<grid, block, h->smem_assign, h->stream>>>(g, h->spins, h->labels, h->rng_state, h->rng_sel,
-                                                            h->rng_iter, accept_threshold(p_add), h->edge, dbg_bonds,
-                                                            dbg_assign);
+    k_assign<W, TXc, TYc, kDebug><<<grid, block, h->smem_assign, h->stream>>>(
+        g, h->spins, h->labels, h->rng_state, h->rng_sel, h->rng_iter, accept_threshold(p_add), h->edge, dbg_bonds,
+        dbg_assign);
     SWB_LAUNCHED();
     return SWB_OK;
+}
+
+template <int W>
+int launch_assign_w(swb_lattice *h, float p_add, uint8_t *dbg_bonds, uint32_t *dbg_assign)
+{
+    if (dbg_assign)
+        return launch_assign_k<W, 0, 0, true>(h, p_add, dbg_bonds, dbg_assign);
+    if (W == 16) {
+        const uint32_t tx = h->g.TX, ty = h->g.TY;
+        if (tx == 16 && ty == 8) return launch_assign_k<W, 16, 8, false>(h, p_add, nullptr, nullptr);
+        if (tx == 8 && ty == 8) return launch_assign_k<W, 8, 8, false>(h, p_add, nullptr, nullptr);
+        if (tx == 32 && ty == 4) return launch_assign_k<W, 32, 4, false>(h, p_add, nullptr, nullptr);
+        if (tx == 16 && ty == 16) return launch_assign_k<W, 16, 16, false>(h, p_add, nullptr, nullptr);
+        if (tx == 8 && ty == 16) return launch_assign_k<W, 8, 16, false>(h, p_add, nullptr, nullptr);
+        if (tx == 32 && ty == 8) return launch_assign_k<W, 32, 8, false>(h, p_add, nullptr, nullptr);
+        if (tx == 16 && ty == 4) return launch_assign_k<W, 16, 4, false>(h, p_add, nullptr, nullptr);
+    }
+    return launch_assign_k<W, 0, 0, false>(h, p_add, nullptr, nullptr);
 }
 
 int launch_assign(swb_lattice *h, float p_add, uint8_t *dbg_bonds, uint32_t *dbg_assign)
