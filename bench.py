@@ -114,6 +114,10 @@ class ClockSampler:
                  "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 3.0:   # first sample before timing starts
+                time.sleep(0.02)
+            self.lines.clear()
         except (OSError, FileNotFoundError):
             self.proc = None
         return self
@@ -485,8 +489,8 @@ def bench_batched(args, dist: Dist, cp) -> dict:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="batched", choices=["batched", *PLAIN])
     ap.add_argument("--no-cpu-baseline", action="store_true")
