@@ -387,9 +387,11 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
         // Row requests: tile_x numbers each, x-bond rows then y-bond rows; element k is lane
         // k % W after update k / W + 1 of the request.  The ballot gives every lane the whole
         // word; one lane stores it.
+#pragma unroll
         for (uint32_t req = 0; req < 2 * TY - 1; ++req) {
             const bool upd = req < nrow;
             uint32_t word = 0;
+#pragma unroll
             for (uint32_t sub = 0; sub < Ur; ++sub) {
                 advance(upd);
                 const bool bit = upd && sub * W + lane < TX && lcg_accept(st, thr);
@@ -404,6 +406,7 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
         }
         // The merge request: tile_x + tile_y numbers, [0, tile_x) bottom edge, then right edge.
         uint64_t mbits = 0;
+#pragma unroll
         for (uint32_t sub = 0; sub < Um; ++sub) {
             advance(on);
             const bool bit = on && sub * W + lane < TX + TY && lcg_accept(st, thr);
