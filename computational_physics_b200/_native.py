@@ -59,6 +59,7 @@ _SIGNATURES = {
     "swb_sweep_timed": ([P, F32, U32, I32, P], I32),
     "swb_host_alloc": ([P, ctypes.c_size_t], I32),
     "swb_host_free": ([P], I32),
+    "swb_sweep_static": ([P, U32, U32, U32, U32, U32, F32, U32, P, P, P, P, I32], I32),
 }
 
 

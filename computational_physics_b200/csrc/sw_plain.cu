@@ -34,6 +34,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -778,6 +779,126 @@ int swb_update_host(swb_lattice *h, float temperature, const uint8_t *spins_in, 
         em_out[1] = (double)o.last_m / (double)h->n;
     }
     SWB_CUDA(cudaStreamSynchronize(h->stream));
+    return SWB_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// Sweeps that allocate nothing.
+//
+// Who cannot allocate: a host that keeps the lattice in device memory it manages itself -- the
+// reference's Lattice<2> storage handed over through an FFI, or a serving process whose lattice
+// pool already holds its whole HBM budget.  For such a caller a per-sweep cudaMalloc can fail
+// (the pool has the memory) and a cudaFree synchronises the whole device, stalling the other
+// lattices' streams.  The caller passes its spins and lcg32 streams; the sweep's scratch (label
+// array, block edge words, fault word) lives in the one file-scope device array below, which
+// every call on a device shares.
+
+namespace swb {
+
+constexpr uint64_t kStaticMaxSites = 1ull << 22;               // 2048 x 2048 sites
+constexpr size_t kStaticScratchBytes = (24ull << 20) + 1024;   // labels 16 MiB + edge words + fault
+
+inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+}  // namespace swb
+
+// In host code this name is a stand-in for the array, not a device address: the address comes
+// from cudaGetSymbolAddress, once per device.
+static __device__ __align__(256) unsigned char swb_static_scratch[swb::kStaticScratchBytes];
+
+namespace {
+
+constexpr int kStaticMaxDevices = 64;
+std::mutex g_static_mutex;
+unsigned char *g_static_base[kStaticMaxDevices] = {};
+
+// Device address of swb_static_scratch on the current device (looked up on the first call).
+int static_scratch(int device, unsigned char **base)
+{
+    if (device < 0 || device >= kStaticMaxDevices)
+        return fail(SWB_ERR_ARGUMENT, "device %d out of range", device);
+    std::lock_guard<std::mutex> lock(g_static_mutex);
+    if (!g_static_base[device]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, swb_static_scratch);
+        if (e != cudaSuccess)
+            return fail(SWB_ERR_CUDA, "cudaGetSymbolAddress(swb_static_scratch) on device %d: %s", device,
+                        cudaGetErrorString(e));
+        g_static_base[device] = static_cast<unsigned char *>(p);
+    }
+    *base = g_static_base[device];
+    return SWB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int swb_sweep_static(void *stream, uint32_t L0, uint32_t L1, uint32_t tile_x, uint32_t tile_y, uint32_t lcg_width,
+                     float temperature, uint32_t n_sweeps, uint8_t *spins, uint32_t *rng_state, uint8_t *rng_sel,
+                     uint32_t *rng_iter, int wait)
+{
+    // Every argument is checked before the first CUDA call.
+    if (!spins || !rng_state || !rng_sel || !rng_iter)
+        return fail(SWB_ERR_ARGUMENT, "NULL buffer");
+    if (reinterpret_cast<uintptr_t>(spins) % 16 || reinterpret_cast<uintptr_t>(rng_state) % 4 ||
+        reinterpret_cast<uintptr_t>(rng_iter) % 4)
+        return fail(SWB_ERR_ARGUMENT, "spins must be 16-byte aligned, rng_state and rng_iter 4-byte aligned");
+    if (L0 == 0 || L1 == 0 || (L0 % 2) || (L1 % 2))
+        return fail(SWB_ERR_ARGUMENT, "SwendsenWang_2D implementation requires evenly sized lattice (%u x %u)", L0, L1);
+    if ((uint64_t)L0 * L1 > kStaticMaxSites)
+        return fail(SWB_ERR_CAPACITY, "lattice of %u x %u sites exceeds the static scratch limit of %llu sites", L0, L1,
+                    (unsigned long long)kStaticMaxSites);
+    if (!(tile_x == 8 || tile_x == 16 || tile_x == 32) || tile_y < 2 || tile_y > 32)
+        return fail(SWB_ERR_ARGUMENT, "unsupported tile %u x %u (tile_x in {8,16,32}, 2 <= tile_y <= 32)", tile_x, tile_y);
+    if (!valid_width(lcg_width))
+        return fail(SWB_ERR_ARGUMENT, "unsupported lcg32 width %u (8, 16 or 32)", lcg_width);
+    if (!(temperature > 0.0f) || !std::isfinite(temperature))
+        return fail(SWB_ERR_ARGUMENT, "temperature must be positive and finite");
+
+    swb_lattice h;  // a view: caller's buffers plus the static scratch; owns nothing
+    h.stream = static_cast<cudaStream_t>(stream);
+    h.W = lcg_width;
+    h.g = make_geo(L0, L1, tile_x, tile_y, lcg_width, kAssignThreads);
+    h.n = (size_t)L0 * L1;
+    h.n_tiles = h.g.n0 * h.g.n1;
+    h.n_blocks = h.g.nbx * h.g.nby;
+    h.smem_assign = assign_smem(h.g).total;
+    h.smem_flip = flip_smem_bytes(h.g);
+    const size_t labels_bytes = align256(h.n * sizeof(uint32_t) + 16);
+    const size_t edge_bytes = align256((size_t)h.n_blocks * kEdgeWords * sizeof(uint32_t));
+    if (labels_bytes + edge_bytes + 256 > kStaticScratchBytes)
+        return fail(SWB_ERR_CAPACITY, "lattice %u x %u with tile %u x %u needs %zu bytes of scratch, the static array holds %zu",
+                    L0, L1, tile_x, tile_y, labels_bytes + edge_bytes + 256, kStaticScratchBytes);
+
+    SWB_CUDA(cudaGetDevice(&h.device));
+    unsigned char *base = nullptr;
+    if (int rc = static_scratch(h.device, &base))
+        return rc;
+    h.spins = spins;
+    h.rng_state = rng_state;
+    h.rng_sel = rng_sel;
+    h.rng_iter = rng_iter;
+    h.labels = reinterpret_cast<uint32_t *>(base);
+    h.edge = reinterpret_cast<uint32_t *>(base + labels_bytes);
+    h.fault = reinterpret_cast<unsigned int *>(base + labels_bytes + edge_bytes);
+
+    // The array keeps the previous call's contents.  Labels and edge words are fully written by
+    // the assign kernel before they are read; only the fault word must start at zero.
+    SWB_CUDA(cudaMemsetAsync(h.fault, 0, sizeof(unsigned int), h.stream));
+    const float p_add = swb_p_add(temperature);
+    for (uint32_t s = 0; s < n_sweeps; ++s)
+        if (int rc = launch_sweep(&h, p_add, false, nullptr, nullptr))
+            return rc;
+    if (wait) {
+        unsigned int f = 0;
+        SWB_CUDA(cudaMemcpyAsync(&f, h.fault, sizeof(f), cudaMemcpyDeviceToHost, h.stream));
+        SWB_CUDA(cudaStreamSynchronize(h.stream));
+        if (f)
+            return fail(SWB_ERR_STATE, "label chase exceeded %u steps (fault word %u)", kChainCap, f);
+    }
     return SWB_OK;
 }
 

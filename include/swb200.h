@@ -147,6 +147,25 @@ int swb_host_free(void *ptr);
 int swb_update_host(swb_lattice *h, float temperature, const uint8_t *spins_in, uint8_t *spins_out,
                     double *em_out);
 
+/* No counterpart in the reference.  n_sweeps sweeps of a lattice whose buffers the CALLER owns,
+ * allocating nothing: for hosts that keep the lattice in device memory they manage themselves
+ * (an FFI caller's own lattice storage, a pool holding the whole HBM budget), where a per-call
+ * cudaMalloc can fail and a cudaFree would synchronise the device.  Device buffers, on the
+ * current device: spins[L0*L1] (0/1, 16-byte aligned), rng_state[n_tiles*W], rng_sel[n_tiles*W]
+ * (index 0..4 of the lcg32 parameter pair, random/src/lcg32.cpp:128-135), rng_iter[n_tiles],
+ * n_tiles = ceil(L0/tile_x) * ceil(L1/tile_y) -- the layout swb_get_rng exports.  Results equal
+ * swb_sweep's on the same state.  The label array, block edge words and fault word live in one
+ * static device array of 24 MiB + 1 KiB, so L0*L1 is at most 4,194,304 (2048 x 2048); larger
+ * lattices return SWB_ERR_CAPACITY before any CUDA call.  All calls on a device share that array
+ * (each call clears its fault word, the kernels overwrite the rest): calls that overlap on the
+ * GPU race, so serialise them (one stream, or events).  The first call on each device looks the
+ * array's address up (cudaGetSymbolAddress, with that device current); make that first call
+ * before any stream capture.  Asynchronous on `stream` (NULL = default stream); with wait != 0
+ * the call synchronises the stream and reports a label-chase fault as SWB_ERR_STATE. */
+int swb_sweep_static(void *stream, uint32_t L0, uint32_t L1, uint32_t tile_x, uint32_t tile_y, uint32_t lcg_width,
+                     float temperature, uint32_t n_sweeps, uint8_t *spins, uint32_t *rng_state, uint8_t *rng_sel,
+                     uint32_t *rng_iter, int wait);
+
 /* ---- batched lattices: many independent lattices advanced by one persistent kernel per
  * sweep phase, replayed as a CUDA graph.  No counterpart in the reference, whose
  * Lattice<2>::Update holds one static strategy per process (ising/include/lattice.hpp:51-57);
