@@ -172,6 +172,15 @@ def assign_bytes(n_sites: int, n_tiles: int, W: int) -> float:
     return n_sites * 5 + n_tiles * 2 * (W * 5 + 4)
 
 
+# DRAM traffic of one assign launch (dram__bytes_read.sum + dram__bytes_write.sum) from one ncu
+# capture of the same kernel, per site: the batched mix of 512 lattices (39,603,200 sites:
+# 66,431,744 B read + 182,641,664 B written) and one 8192 x 8192 lattice, tile 16 x 8
+# (125,124,352 B read + 275,793,152 B written).  Traffic grows with the sites swept, so other
+# sizes scale by their site count.
+ASSIGN_TRAFFIC_PER_SITE = {"kb_assign": (66_431_744 + 182_641_664) / 39_603_200,
+                           "k_assign": (125_124_352 + 275_793_152) / 8192 ** 2}
+
+
 def flip_bytes(n_sites: int) -> float:
     """k_flip: labels read (4 B/site) + spins read and written (2 B/site)."""
     return n_sites * 6
@@ -352,8 +361,9 @@ def bench_plain(args, dist: Dist, cp) -> dict:
     return {
         "value": value, "ms_per_step": ms_max / args.steps, "launches": launches, "clocks": clocks.summary(),
         "roofline": {"bound": "hbm", "kernel": "k_assign", "achieved": ab / (a_ms / 1e3) / 1e9, "peak": peak,
-                     "unit": "GB/s", "frac": ab / (a_ms / 1e3) / 1e9 / peak, "traffic": None,
-                     "peak_kind": peak_kind, "bytes_per_launch": ab, "ms_per_launch": a_ms},
+                     "unit": "GB/s", "frac": ab / (a_ms / 1e3) / 1e9 / peak,
+                     "traffic": ASSIGN_TRAFFIC_PER_SITE["k_assign"] * n, "peak_kind": peak_kind,
+                     "bytes_per_launch": ab, "ms_per_launch": a_ms},
         "kernels_ms_per_sweep": {"assign": a_ms, "merge": float(k[2]) / nk, "flip": float(k[3]) / nk},
         "flip_GBs": fb / (float(k[3]) / nk / 1e3) / 1e9,
         "e2e": {"value": e2e, "unit": "spin-updates/s", "h2d_bytes_per_step": n, "d2h_bytes_per_step": n + 16},
@@ -470,7 +480,8 @@ def bench_batched(args, dist: Dist, cp) -> dict:
     res = {
         "value": value, "ms_per_step": ms_max / args.steps, "launches": launches, "clocks": clocks.summary(),
         "roofline": {"bound": "hbm", "kernel": "kb_assign", "achieved": ab / (a_ms / 1e3) / 1e9, "peak": peak,
-                     "unit": "GB/s", "frac": ab / (a_ms / 1e3) / 1e9 / peak, "traffic": None, "peak_kind": peak_kind,
+                     "unit": "GB/s", "frac": ab / (a_ms / 1e3) / 1e9 / peak,
+                     "traffic": ASSIGN_TRAFFIC_PER_SITE["kb_assign"] * sites, "peak_kind": peak_kind,
                      "bytes_per_launch": ab, "ms_per_launch": a_ms},
         "kernels_ms_per_sweep": {"assign": a_ms, "merge": float(k[2]) / nk, "flip": float(k[3]) / nk},
         "e2e": {"value": dist.world * sites * e2e_steps / e2e_s, "unit": "spin-updates/s",
