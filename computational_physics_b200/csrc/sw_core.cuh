@@ -135,6 +135,21 @@ struct LatView {
     uint32_t thr;  // bond accept threshold, accept_threshold(p_add)
 };
 
+// Bit k of the result = bit 0 of byte k of v: multiplying the masked bytes by
+// 2^28 + 2^21 + 2^14 + 2^7 lands byte k's bit at bit 28 + k, every cross term below bit 28.
+__device__ __forceinline__ uint32_t spin_nibble(uint32_t v)
+{
+    return ((v & 0x01010101u) * 0x10204080u) >> 28;
+}
+
+// Bit k = staged spin byte p[k] (0/1) for k < 32; p is 16-byte aligned in shared memory.
+__device__ __forceinline__ uint32_t spin_bits32(const uint8_t *p)
+{
+    const uint4 a = *reinterpret_cast<const uint4 *>(p), b = *reinterpret_cast<const uint4 *>(p + 16);
+    return spin_nibble(a.x) | spin_nibble(a.y) << 4 | spin_nibble(a.z) << 8 | spin_nibble(a.w) << 12 |
+           spin_nibble(b.x) << 16 | spin_nibble(b.y) << 20 | spin_nibble(b.z) << 24 | spin_nibble(b.w) << 28;
+}
+
 // Labelling of a block whose width is a multiple of 32, from the staged spins (sp) and
 // accepted draws (accX, accY, accM) in shared memory.  Warp-per-row: each 32-site word of a
 // row turns into bond bitmasks by __ballot_sync; every site's parent starts at the first site
@@ -164,53 +179,74 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
     const uint32_t pitch = L.pitch;
     const uint32_t txs = TXc ? (TXc == 8 ? 3 : TXc == 16 ? 4 : 5) : 31 - __clz(TX);  // TX is 8, 16 or 32
 
-    // bond words; edge bonds go to edge_s (right edge: one bit per row, bottom: the row's words)
-    for (uint32_t yl = warp; yl < BY; yl += nwarps) {
-        const uint32_t tby = yl / TY, jj = yl - tby * TY;
-        const uint32_t jjmax = byv > tby * TY ? min(TY, byv - tby * TY) : 0;
-        for (uint32_t w = 0; w < NW; ++w) {
-            const uint32_t xl = (w << 5) + lane;
-            parent[yl * BX + xl] = yl * BX + xl;
-            bool xb = false, yb = false;
-            if (xl < bxv && yl < byv) {
-                const uint32_t tbx = xl >> txs, tb = tby * g.TBX + tbx;
-                const uint32_t ii = xl - (tbx << txs);
-                const uint32_t iimax = min(TX, bxv - (tbx << txs));
-                const uint8_t s = sp[yl * pitch + xl];
-                const uint32_t xa = (ii + 1 < iimax) ? (accX[tb * TY + jj] >> ii) : (uint32_t)(accM[tb] >> (TX + jj));
-                const uint32_t ya = (jj + 1 < jjmax) ? (accY[tb * TY + jj] >> ii) : (uint32_t)(accM[tb] >> ii);
-                xb = (xa & 1u) && s == sp[yl * pitch + xl + 1];
-                yb = (ya & 1u) && s == sp[(yl + 1) * pitch + xl];
+    // Every site starts as its own root (16-byte stores; parent is at offset 0 and BX*BY is a
+    // multiple of 64).
+    for (uint32_t i = tid; i < (BX * BY) >> 2; i += blockDim.x)
+        reinterpret_cast<uint4 *>(parent)[i] = make_uint4(4 * i, 4 * i + 1, 4 * i + 2, 4 * i + 3);
+
+    // Bond words, bit-parallel: one thread per 32-site word of a row.  Spin bits come from the
+    // staged bytes (the word, the word below and the byte to its right: the halo column and
+    // row are staged at column bxv and row byv); a bond needs equal spins and an accepted draw.
+    // Accept bits per tile: x bonds [0, iimax - 1) from the row's x request, the tile's last
+    // column from the merge request's right edge (bit TX + jj); y bonds from the row's y request,
+    // or on the tile's last row from the merge request's bottom edge (bits [0, TX)).  Edge bonds
+    // go to edge_s (right edge: one bit per row, bottom: the row's words).
+    for (uint32_t i = tid; i < BY * NW; i += blockDim.x) {
+        const uint32_t yl = i / NW, w = i - yl * NW;
+        uint32_t X = 0, Y = 0;
+        if (yl < byv) {
+            const uint32_t tby = yl / TY, jj = yl - tby * TY;
+            const uint32_t jjmax = min(TY, byv - tby * TY);
+            const uint8_t *row = sp + yl * pitch + (w << 5);
+            const uint32_t S = spin_bits32(row), D = spin_bits32(row + pitch);
+            const uint32_t R = __funnelshift_r(S, (uint32_t)row[32], 1);  // right neighbours
+            uint32_t AX = 0, AY = 0;
+            constexpr uint32_t kTiles = TXc ? 32 / TXc : 4;
+            const uint32_t tiles = TXc ? kTiles : 32 >> txs;
+#pragma unroll
+            for (uint32_t k = 0; k < kTiles; ++k) {
+                const uint32_t c0 = (w << 5) + (k << txs);  // the tile's first column in the block
+                if (k < tiles && c0 < bxv) {
+                    const uint32_t tb = tby * g.TBX + (c0 >> txs);
+                    const uint32_t iimax = min(TX, bxv - c0);
+                    const uint32_t tmask = 0xFFFFFFFFu >> (32 - iimax);
+                    const uint64_t am = accM[tb];
+                    const uint32_t xb = (accX[tb * TY + jj] & (tmask >> 1)) | ((uint32_t)(am >> (TX + jj)) & 1u) << (iimax - 1);
+                    const uint32_t yb = (jj + 1 < jjmax ? accY[tb * TY + jj] : (uint32_t)am) & tmask;
+                    AX |= xb << (k << txs);
+                    AY |= yb << (k << txs);
+                }
             }
-            uint32_t X = __ballot_sync(0xffffffffu, xb), Y = __ballot_sync(0xffffffffu, yb);
-            if (lane == 0) {
-                if (bxv - 1 - (w << 5) < 32u) {  // the block's last column lies in this word
-                    const uint32_t bit = (bxv - 1) & 31;
-                    if ((X >> bit) & 1u)
-                        atomicOr(edge_s, 1u << yl);
-                    X &= ~(1u << bit);
-                }
-                if (yl + 1 == byv) {
-                    edge_s[1 + w] = Y;
-                    Y = 0;
-                }
-                Xw[yl * NW + w] = X;
-                Yw[yl * NW + w] = Y;
+            X = ~(S ^ R) & AX;
+            Y = ~(S ^ D) & AY;
+            if (bxv - 1 - (w << 5) < 32u) {  // the block's last column lies in this word
+                const uint32_t bit = (bxv - 1) & 31;
+                if ((X >> bit) & 1u)
+                    atomicOr(edge_s, 1u << yl);
+                X &= ~(1u << bit);
+            }
+            if (yl + 1 == byv) {
+                edge_s[1 + w] = Y;
+                Y = 0;
             }
         }
+        Xw[yl * NW + w] = X;
+        Yw[yl * NW + w] = Y;
     }
     __syncthreads();
 
     // Scanline labelling.  Work item = (32-column strip, band of rows); a warp walks its band
     // top-down with each lane holding the provisional label of the site above.  A run (x-bonded
-    // sites of the strip row, found from the gap mask) takes the minimum of the labels reaching
-    // it through y-bonds -- a segmented min over the run by five shfl_up steps -- or, with none,
-    // its own first site as a new label.  Two different labels meeting in a run are united in
-    // the shared union-find (toward the minimum).  Seams between strips and bands are united
-    // afterwards, then every site resolves its provisional label.
+    // sites of the strip row; its first lane from the gap mask below the lane, its last from the
+    // gap mask above) takes the label above its leftmost y-bonded site, or with none its own first
+    // site as a new label.  Every other y-bond of the run that meets a different label unites the
+    // two in the shared union-find (toward the minimum), so each site's root is the minimum of
+    // its block-local component.  Seams between strips and bands are united afterwards, then
+    // every site resolves its provisional label.
     uint16_t *plab = reinterpret_cast<uint16_t *>(smem + L.plab);
     const uint32_t nb = max(1u, nwarps / NW);                // bands
     const uint32_t rb = (BY + nb - 1) / nb;                  // rows per band
+    const uint32_t below = (1u << lane) - 1u;                // lanes below this one
     for (uint32_t task = warp; task < NW * nb; task += nwarps) {
         const uint32_t sx = task % NW, band = task / NW;
         const uint32_t ya = band * rb, yb = min(BY, ya + rb);
@@ -218,22 +254,16 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
         for (uint32_t yl = ya; yl < yb; ++yl) {
             const uint32_t X = Xw[yl * NW + sx];
             const uint32_t Yup = yl > ya ? Yw[(yl - 1) * NW + sx] : 0u;
-            const uint32_t gaps = ~X & ((1u << lane) - 1u);
-            const uint32_t rs = gaps ? 32 - __clz(gaps) : 0;            // run start (lane)
-            const uint32_t re = __ffs(~X & (0xFFFFFFFFu << lane)) - 1;   // run end (lane); X bit 31 never ends a strip run
-            const bool up = (Yup >> lane) & 1u;
-            uint32_t c = up ? above : 0xFFFFFFFFu;
-#pragma unroll
-            for (uint32_t d = 1; d < 32; d <<= 1) {
-                const uint32_t v = __shfl_up_sync(0xffffffffu, c, d);
-                if (lane >= rs + d)
-                    c = min(c, v);
-            }
-            const uint32_t m = __shfl_sync(0xffffffffu, c, re == 0xFFFFFFFFu ? 31 : re);
-            const uint32_t lab = m != 0xFFFFFFFFu ? m : yl * BX + (sx << 5) + rs;
-            if (up && above != lab)
+            const uint32_t rs = 32 - __clz(~X & below);             // run start (lane); __clz(0) = 32
+            const uint32_t from = 0xFFFFFFFFu << rs;
+            const uint32_t re = (__ffs(~X & from) - 1) & 31u;        // run end; X bit 31 never ends a strip run
+            const uint32_t f = __ffs(Yup & from) - 1;               // leftmost y-bond from the run start, or ~0
+            const uint32_t rep = __shfl_sync(0xffffffffu, above, f & 31u);
+            const uint32_t base = yl * BX + (sx << 5);
+            const uint32_t lab = f <= re ? rep : base + rs;
+            if (((Yup >> lane) & 1u) && above != lab)
                 uf_union(parent, above, lab);
-            plab[yl * BX + (sx << 5) + lane] = (uint16_t)lab;
+            plab[base + lane] = (uint16_t)lab;
             above = lab;
         }
     }
