@@ -151,11 +151,8 @@ __device__ __forceinline__ uint32_t spin_bits32(const uint8_t *p)
 }
 
 // Labelling of a block whose width is a multiple of 32, from the staged spins (sp) and
-// accepted draws (accX, accY, accM) in shared memory.  Warp-per-row: each 32-site word of a
-// row turns into bond bitmasks by __ballot_sync; every site's parent starts at the first site
-// of its x-bonded run (a run's minimum, found with __clz on the gap mask), so horizontal
-// bonds need no union; a vertical bond is united only when the bond to its left does not
-// already join the same two runs.  The result equals the generic path's: the minimum site
+// accepted draws (accX, accY, accM) in shared memory: bond bitmasks per 32-site word, then a
+// scanline pass over x-runs (below).  The result equals the generic path's: the minimum site
 // index of each block-local component.
 template <int TXc, int TYc>
 __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uint32_t bxi, const uint32_t byi,
@@ -414,6 +411,79 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
                 to_rot = rot ? kShuffleDistance : to_rot - 1;
             }
         };
+        // Full-height tiles with a compile-time shape (every tile of the warp that lies on the
+        // lattice has tile_y rows): the same sequence with the update count known at every
+        // step, so nothing is predicated; lane r % W of a tile keeps request r's word in a
+        // register and stores it after the loop.  Segments of tiles off the lattice run along
+        // and store nothing.
+        bool fast = false;
+        if constexpr (TXc != 0 && TYc != 0) {
+            if (__all_sync(0xffffffffu, !on || jjmax == TYc)) {
+                constexpr uint32_t kReq = 2 * TYc - 1, kWpl = (kReq + W - 1) / W;
+                constexpr uint32_t kUr = (TXc + W - 1) / W, kUm = (TXc + TYc + W - 1) / W;
+                uint32_t words[kWpl];
+#pragma unroll
+                for (uint32_t k = 0; k < kWpl; ++k)
+                    words[k] = 0;
+                // Update number k + 1 of this sweep (k compile-time after unrolling).
+                auto step = [&](const uint32_t k) {
+                    const bool rot = to_rot == 1;
+                    if (__any_sync(0xffffffffu, rot)) {
+                        const uint32_t itn = it + k + 1;
+                        const uint32_t src = __shfl_sync(0xffffffffu, st, itn & (W - 1), W);
+                        const uint32_t from = (lane + src + ((itn & 1u) ? 0u : 1u)) & (W - 1);
+                        const uint32_t a2 = __shfl_sync(0xffffffffu, a, from, W);
+                        const uint32_t c2 = __shfl_sync(0xffffffffu, c, from, W);
+                        const uint32_t s2 = __shfl_sync(0xffffffffu, sel, from, W);
+                        if (rot) {
+                            a = a2;
+                            c = c2;
+                            sel = s2;
+                        }
+                    }
+                    st = a * st + c;
+                    to_rot = rot ? kShuffleDistance : to_rot - 1;
+                };
+#pragma unroll
+                for (uint32_t req = 0; req < kReq; ++req) {
+                    uint32_t word = 0;
+#pragma unroll
+                    for (uint32_t sub = 0; sub < kUr; ++sub) {
+                        step(req * kUr + sub);
+                        const bool bit = sub * W + lane < TXc && lcg_accept(st, thr);
+                        word |= ((__ballot_sync(0xffffffffu, bit) >> seg_shift) & seg_mask) << (sub * W);
+                    }
+                    if (lane == req % W)
+                        words[req / W] = word;
+                }
+                uint64_t mbits = 0;
+#pragma unroll
+                for (uint32_t sub = 0; sub < kUm; ++sub) {
+                    step(kReq * kUr + sub);
+                    const bool bit = sub * W + lane < TXc + TYc && lcg_accept(st, thr);
+                    mbits |= (uint64_t)((__ballot_sync(0xffffffffu, bit) >> seg_shift) & seg_mask) << (sub * W);
+                }
+                it += kReq * kUr + kUm;
+                if (on) {
+#pragma unroll
+                    for (uint32_t k = 0; k < kWpl; ++k) {
+                        const uint32_t req = lane + k * W;
+                        if (req < TYc)
+                            accX[tb * TYc + req] = words[k];
+                        else if (req < kReq)
+                            accY[tb * TYc + req - TYc] = words[k];
+                    }
+                    rng_state[(size_t)tile * W + lane] = st;
+                    rng_sel[(size_t)tile * W + lane] = (uint8_t)sel;
+                    if (lane == 0)
+                        rng_iter[tile] = it;
+                }
+                if (lane == 0 && tb < ntb)
+                    accM[tb] = on ? mbits : 0;
+                fast = true;
+            }
+        }
+        if (!fast) {
         // Row requests: tile_x numbers each, x-bond rows then y-bond rows; element k is lane
         // k % W after update k / W + 1 of the request.  The ballot gives every lane the whole
         // word; one lane stores it.
@@ -450,6 +520,7 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
         }
         if (lane == 0 && tb < ntb)
             accM[tb] = mbits;
+        }
     }
     asm volatile("cp.async.wait_all;\n" ::: "memory");
     if (tid < byv)
