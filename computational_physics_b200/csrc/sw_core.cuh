@@ -676,7 +676,7 @@ __device__ __forceinline__ void merge_block(const Geo &g, const uint32_t blk, co
         const volatile uint32_t *vl = labels;
         const uint32_t a = label_global(g, bxi, byi, vl[s]), b = label_global(g, nbx, nby, vl[nb]);
         if (a != b)
-            guf_union(labels, a, b, fault);
+            guf_union_pair(labels, a, b, fault);
     }
 }
 
@@ -724,8 +724,8 @@ __device__ __forceinline__ void flip_block(const Geo &g, const uint32_t bxi, con
                 const uint32_t v[4] = {lab[k].x, lab[k].y, lab[k].z, lab[k].w};
 #pragma unroll
                 for (int j = 0; j < 4; ++j)
-                    if (!(v[j] & kLocalFlag))
-                        res[lidx[k] + j] = guf_find(labels, sidx[k] + j, fault);
+                    if (!(v[j] & kLocalFlag))  // a block root: v is its parent (itself unless merged)
+                        res[lidx[k] + j] = v[j] == sidx[k] + j ? v[j] : guf_find(labels, v[j], fault);
             }
         }
         __syncthreads();
@@ -749,8 +749,9 @@ __device__ __forceinline__ void flip_block(const Geo &g, const uint32_t bxi, con
     for (uint32_t yl = warp; yl < byv; yl += nwarps)
         for (uint32_t xl = lane; xl < bxv; xl += 32) {
             const uint32_t site = base + yl * L0 + xl;
-            if (!(labels[site] & kLocalFlag))
-                res[yl * BX + xl] = guf_find(labels, site, fault);
+            const uint32_t v = labels[site];
+            if (!(v & kLocalFlag))
+                res[yl * BX + xl] = v == site ? v : guf_find(labels, v, fault);
         }
     __syncthreads();
     if ((L0 & 3u) == 0) {

@@ -182,4 +182,47 @@ __device__ __forceinline__ void guf_union(uint32_t *p, uint32_t a, uint32_t b, u
     atomicOr(fault, 2u);
 }
 
+// The same union with the two root walks advancing together, one level per step, so the loads
+// of both chains are in flight at once.  Each step also points the node it leaves at its
+// grandparent (path splitting, by atomicMin as above).  Same caps and fault bits.
+__device__ __forceinline__ void guf_union_pair(uint32_t *p, uint32_t a, uint32_t b, unsigned int *fault)
+{
+    const volatile uint32_t *vp = p;
+    for (uint32_t n = 0; n < kUnionRetryCap; ++n) {
+        uint32_t ya = vp[a], yb = vp[b];
+        for (uint32_t k = 0; ya != a || yb != b; ++k) {
+            if (k >= kChainCap) {
+                atomicOr(fault, 1u);
+                return;
+            }
+            const uint32_t za = ya != a ? vp[ya] : ya;
+            const uint32_t zb = yb != b ? vp[yb] : yb;
+            if (ya != a) {
+                if (za != ya)
+                    atomicMin(p + a, za);
+                a = ya;
+                ya = za;
+            }
+            if (yb != b) {
+                if (zb != yb)
+                    atomicMin(p + b, zb);
+                b = yb;
+                yb = zb;
+            }
+        }
+        if (a == b)
+            return;
+        if (a > b) {
+            const uint32_t t = a;
+            a = b;
+            b = t;
+        }
+        const uint32_t old = atomicMin(p + b, a);
+        if (old == b)
+            return;
+        b = old;
+    }
+    atomicOr(fault, 2u);
+}
+
 }  // namespace swb
