@@ -691,7 +691,7 @@ __host__ __device__ inline uint32_t flip_smem_bytes(const Geo &g)
 // blocks) into shared memory; every site then reads its root's result there and flips iff the
 // cluster's label is odd.  kWriteLabels stores the resolved global labels (the reference's
 // ResolveLabels output).
-template <bool kWriteLabels>
+template <bool kWriteLabels, int kQuads = 2>
 __device__ __forceinline__ void flip_block(const Geo &g, const uint32_t bxi, const uint32_t byi, uint8_t *spins,
                                            uint32_t *labels, unsigned int *fault, unsigned char *smem)
 {
@@ -702,46 +702,50 @@ __device__ __forceinline__ void flip_block(const Geo &g, const uint32_t bxi, con
     const uint32_t bxv = min(BX, L0 - x0), byv = min(g.BY, g.L1 - y0);
     const uint32_t base = y0 * L0 + x0;
     const uint32_t nq = (bxv >> 2) * byv, qrow = bxv >> 2;
-    if ((L0 & 3u) == 0 && nq <= 2 * blockDim.x) {
-        // Every thread holds at most two quads (4 labels + 4 spins each) in registers: one
-        // round trip for the loads, the roots' chains, then the flips.
-        uint4 lab[2];
-        uint32_t spn[2], sidx[2], lidx[2];
+    if ((L0 & 3u) == 0 && qrow && blockDim.x % qrow == 0 && nq <= kQuads * blockDim.x) {
+        // Every thread holds at most kQuads quads (4 labels + 4 spins each) in registers: one
+        // round trip for the loads, the merged roots' chains, then the flips.  Quad k of a
+        // thread is column xq of row yl0 + k * rstep (whole rows per step, so no division).
+        const uint32_t rstep = blockDim.x / qrow, yl0 = tid / qrow, xq4 = 4 * (tid - yl0 * qrow);
+        uint4 lab[kQuads];
+        uint32_t spn[kQuads];
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const uint32_t qi = tid + k * blockDim.x;
-            if (qi < nq) {
-                const uint32_t yl = qi / qrow, xq = qi - yl * qrow;
-                sidx[k] = base + yl * L0 + 4 * xq;
-                lidx[k] = yl * BX + 4 * xq;
-                lab[k] = *reinterpret_cast<const uint4 *>(labels + sidx[k]);
-                spn[k] = reinterpret_cast<const uint32_t *>(spins)[sidx[k] >> 2];
+        for (int k = 0; k < kQuads; ++k) {
+            const uint32_t yl = yl0 + k * rstep;
+            if (yl < byv) {
+                const uint32_t s = base + yl * L0 + xq4;
+                lab[k] = *reinterpret_cast<const uint4 *>(labels + s);
+                spn[k] = reinterpret_cast<const uint32_t *>(spins)[s >> 2];
             }
         }
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            if (tid + k * blockDim.x < nq) {
+        for (int k = 0; k < kQuads; ++k) {
+            const uint32_t yl = yl0 + k * rstep;
+            if (yl < byv) {
+                const uint32_t s = base + yl * L0 + xq4, l = yl * BX + xq4;
                 const uint32_t v[4] = {lab[k].x, lab[k].y, lab[k].z, lab[k].w};
 #pragma unroll
                 for (int j = 0; j < 4; ++j)
                     if (!(v[j] & kLocalFlag))  // a block root: v is its parent (itself unless merged)
-                        res[lidx[k] + j] = v[j] == sidx[k] + j ? v[j] : guf_find(labels, v[j], fault);
+                        res[l + j] = v[j] == s + j ? v[j] : guf_find(labels, v[j], fault);
             }
         }
         __syncthreads();
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            if (tid + k * blockDim.x < nq) {
+        for (int k = 0; k < kQuads; ++k) {
+            const uint32_t yl = yl0 + k * rstep;
+            if (yl < byv) {
+                const uint32_t s = base + yl * L0 + xq4, l = yl * BX + xq4;
                 const uint32_t v[4] = {lab[k].x, lab[k].y, lab[k].z, lab[k].w};
                 uint32_t r[4], flip = 0;
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
-                    r[j] = res[(v[j] & kLocalFlag) ? (v[j] & kLocalMask) : lidx[k] + j];
+                    r[j] = res[(v[j] & kLocalFlag) ? (v[j] & kLocalMask) : l + j];
                     flip |= (r[j] & 1u) << (8 * j);
                 }
-                reinterpret_cast<uint32_t *>(spins)[sidx[k] >> 2] = spn[k] ^ flip;
+                reinterpret_cast<uint32_t *>(spins)[s >> 2] = spn[k] ^ flip;
                 if (kWriteLabels)
-                    *reinterpret_cast<uint4 *>(labels + sidx[k]) = make_uint4(r[0], r[1], r[2], r[3]);
+                    *reinterpret_cast<uint4 *>(labels + s) = make_uint4(r[0], r[1], r[2], r[3]);
             }
         }
         return;

@@ -83,14 +83,14 @@ __global__ void __launch_bounds__(256) k_merge(const Geo g, const uint32_t *__re
 }
 
 // Resolve + flip, one CTA per block (flip_block).
-constexpr uint32_t kFlipThreads = 512;
+constexpr uint32_t kFlipThreads = 256;  // 6 CTAs per SM (40 registers), four quads of a 128 x 32 block per thread
 
 template <bool kWriteLabels>
-__global__ void __launch_bounds__(kFlipThreads) k_flip(const Geo g, uint8_t *__restrict__ spins, uint32_t *labels,
+__global__ void __launch_bounds__(kFlipThreads, 6) k_flip(const Geo g, uint8_t *__restrict__ spins, uint32_t *labels,
                                                        unsigned int *fault)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    flip_block<kWriteLabels>(g, blockIdx.x, blockIdx.y, spins, labels, fault, smem);
+    flip_block<kWriteLabels, 4>(g, blockIdx.x, blockIdx.y, spins, labels, fault, smem);
 }
 
 __global__ void __launch_bounds__(256) k_measure(const uint32_t L0, const uint32_t L1, const uint8_t *__restrict__ spins,
