@@ -26,7 +26,9 @@
 
 namespace swb {
 
-constexpr uint32_t kBatchThreads = 512;        // CTA size of the persistent kernels
+constexpr uint32_t kBatchThreads = 512;        // CTA size of the persistent assign and measure kernels
+constexpr uint32_t kMergeThreads = 192;        // merge: one thread per block edge site (BX + BY <= 160)
+constexpr uint32_t kFlipThreads = 256;         // flip: four quads of a 128 x 32 block per thread
 constexpr uint32_t kChunkSites = 4096;         // measure work item
 constexpr uint32_t kUnlimited = 0xFFFFFFFFu;   // sweeps_left value that never runs out
 
@@ -108,7 +110,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4) kb_assign(BatchLat *lats, co
     }
 }
 
-__global__ void __launch_bounds__(kBatchThreads) kb_merge(BatchLat *lats, const uint32_t *active, const uint32_t *blk_prefix,
+__global__ void __launch_bounds__(kMergeThreads) kb_merge(BatchLat *lats, const uint32_t *active, const uint32_t *blk_prefix,
                                                           BatchCounters *ctr, unsigned int *fault)
 {
     __shared__ uint32_t slot;
@@ -131,7 +133,7 @@ __global__ void __launch_bounds__(kBatchThreads) kb_merge(BatchLat *lats, const 
 
 // Resolve + flip of one block (flip_block); the last block of a lattice closes its round
 // (sweep count and budget).
-__global__ void __launch_bounds__(kBatchThreads) kb_flip(BatchLat *lats, const uint32_t *active, const uint32_t *blk_prefix,
+__global__ void __launch_bounds__(kFlipThreads, 6) kb_flip(BatchLat *lats, const uint32_t *active, const uint32_t *blk_prefix,
                                                          BatchCounters *ctr, unsigned int *fault)
 {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -149,7 +151,7 @@ __global__ void __launch_bounds__(kBatchThreads) kb_flip(BatchLat *lats, const u
             continue;
         const Geo g = L->g;
         const uint32_t blk = item - blk_prefix[k];
-        flip_block<false>(g, blk % g.nbx, blk / g.nbx, L->spins, L->labels, fault, smem);
+        flip_block<false, 4>(g, blk % g.nbx, blk / g.nbx, L->spins, L->labels, fault, smem);
         __syncthreads();
         if (threadIdx.x == 0) {
             __threadfence();
@@ -318,7 +320,7 @@ struct swb_batch {
     unsigned int *d_fault = nullptr;
     std::vector<uint32_t> active;   // ids in the work lists
     bool lists_dirty = true;
-    int grid_assign = 0, grid_other = 0, grid_flip = 0;
+    int grid_assign = 0, grid_other = 0, grid_merge = 0, grid_flip = 0;
     uint32_t smem_assign = 0, smem_flip = 0;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};   // [measure?]
     uint64_t series_cap = 1u << 16;
@@ -403,10 +405,10 @@ int launch_round_w(swb_batch *b, bool measure)
     kb_assign<W><<<b->grid_assign, kBatchThreads, b->smem_assign, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix,
                                                                               b->d_ctr);
     SWB_LAUNCHED();
-    kb_merge<<<b->grid_other, kBatchThreads, 0, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix, b->d_ctr,
+    kb_merge<<<b->grid_merge, kMergeThreads, 0, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix, b->d_ctr,
                                                              b->d_fault);
     SWB_LAUNCHED();
-    kb_flip<<<b->grid_flip, kBatchThreads, b->smem_flip, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix, b->d_ctr,
+    kb_flip<<<b->grid_flip, kFlipThreads, b->smem_flip, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix, b->d_ctr,
                                                                       b->d_fault);
     SWB_LAUNCHED();
     if (measure) {
@@ -535,11 +537,13 @@ int swb_batch_create(swb_batch **out, uint32_t capacity, uint64_t hbm_budget_byt
     }
     b->grid_assign = sms * std::max(per_sm, 1);
     b->smem_flip = flip_smem_bytes(gmax);
-    int per_sm2 = 1, per_sm3 = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, kb_merge, kBatchThreads, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm3, kb_flip, kBatchThreads, b->smem_flip);
-    b->grid_other = sms * std::max(per_sm2, 1);
+    int per_sm2 = 1, per_sm3 = 1, per_sm4 = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, kb_merge, kMergeThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm3, kb_flip, kFlipThreads, b->smem_flip);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm4, kb_measure, kBatchThreads, 0);
+    b->grid_merge = sms * std::max(per_sm2, 1);
     b->grid_flip = sms * std::max(per_sm3, 1);
+    b->grid_other = sms * std::max(per_sm4, 1);
     SWB_TRY(cudaStreamSynchronize(b->stream));
 #undef SWB_TRY
     *out = b;
@@ -809,11 +813,11 @@ int swb_batch_sweep_timed(swb_batch *b, uint32_t n_rounds, int per_kernel, float
             }
             SWB_LAUNCHED();
             SWB_CUDA(cudaEventRecord(ev[2], b->stream));
-            kb_merge<<<b->grid_other, kBatchThreads, 0, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix, b->d_ctr,
+            kb_merge<<<b->grid_merge, kMergeThreads, 0, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix, b->d_ctr,
                                                                      b->d_fault);
             SWB_LAUNCHED();
             SWB_CUDA(cudaEventRecord(ev[3], b->stream));
-            kb_flip<<<b->grid_flip, kBatchThreads, b->smem_flip, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix,
+            kb_flip<<<b->grid_flip, kFlipThreads, b->smem_flip, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix,
                                                                               b->d_ctr, b->d_fault);
             SWB_LAUNCHED();
             SWB_CUDA(cudaEventRecord(ev[4], b->stream));
