@@ -460,14 +460,17 @@ def bench_batched(args, dist: Dist, cp) -> dict:
         n_tiles += b.info(lid)["tiles"]
     ab = assign_bytes(sites, n_tiles, 16)
     peak, peak_kind = hbm_peak()
-    # e2e: every step copies all spins in from pinned host memory and back out
-    ins = []
-    outs = []
+    # e2e: every step copies all spins in from pinned host memory and back out; the lattices'
+    # host buffers are consecutive slices of one pinned arena per direction
+    arena_in = cp.pinned_empty((sites,), np.uint8)
+    arena_out = cp.pinned_empty((sites,), np.uint8)
+    ins, outs, off = [], [], 0
     for lid, (L, _, _) in zip(ids, mix):
-        x = cp.pinned_empty((L, L), np.uint8)
+        x = arena_in[off:off + L * L].reshape(L, L)
         x[:] = b.get_spins(lid)
         ins.append(x)
-        outs.append(cp.pinned_empty((L, L), np.uint8))
+        outs.append(arena_out[off:off + L * L].reshape(L, L))
+        off += L * L
     b.update_host(ids, ins, outs)
     e2e_steps = max(3, min(args.steps, 10))
     dist.barrier()

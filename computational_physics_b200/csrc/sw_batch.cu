@@ -1,13 +1,14 @@
 // Batched Swendsen-Wang: hundreds of independent periodic lattices of different sizes,
 // tiles and temperatures advance together, one persistent kernel per sweep phase.
 //
-// Work queue.  Every active lattice contributes its blocks (TBX x TBY tiles) to one flat list
-// of work items; a lattice's items follow the exclusive prefix sum blk_prefix.  The persistent
-// CTAs of kb_assign / kb_merge / kb_flip pull items from a device counter (atomicAdd) until the
-// list is exhausted; kb_measure does the same over chunks of 4096 sites.  Each phase resets
-// the counter of the phase that ran before it, so a sweep needs no host work and the whole
-// sweep is one CUDA graph, captured once per handle and replayed: the graph reads the item
-// totals from device memory, so adding or removing lattices does not invalidate it.
+// Work items.  Every active lattice contributes its blocks (TBX x TBY tiles) to one flat list
+// of block items (lattice slot, block coordinates), big lattices first.  The persistent CTAs
+// of kb_assign / kb_merge / kb_flip take items blockIdx.x, blockIdx.x + gridDim.x, ... and
+// load the next item's descriptor while they work on the current one; kb_measure pulls chunks
+// of 4096 sites from a device counter (atomicAdd), which kb_assign resets.  A sweep needs no
+// host work and is one CUDA graph, captured once per handle and replayed: the graph reads the
+// item totals from device memory, so adding or removing lattices does not invalidate it (only
+// growing the item list past its allocation does, which re-captures).
 //
 // Per lattice the device keeps spins, labels, lcg32 streams (one per tile, seeded
 // seed_base + tile id as the reference's CPU path with one stream per tile), a sweep budget
@@ -83,86 +84,77 @@ __device__ __forceinline__ uint32_t next_item(unsigned int *queue, uint32_t *slo
     return item;
 }
 
+// Item k of the flat block list: x = lattice slot, y = byi << 16 | bxi.
+__device__ __forceinline__ uint2 load_item(const uint2 *items, uint32_t k, uint32_t total)
+{
+    return k < total ? items[k] : make_uint2(0, 0);
+}
+
 template <int W>
-__global__ void __launch_bounds__(kBatchThreads, 4) kb_assign(BatchLat *lats, const uint32_t *active, const uint32_t *blk_prefix,
-                                                           BatchCounters *ctr)
+__global__ void __launch_bounds__(kBatchThreads, 4) kb_assign(BatchLat *lats, const uint2 *items, BatchCounters *ctr)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ uint32_t slot;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        ctr->queue[2] = 0;  // flip and measure of the previous round are finished
-        ctr->queue[3] = 0;
-    }
-    const uint32_t n = ctr->n_active, total = ctr->total_blocks;
-    while (true) {
-        const uint32_t item = next_item(&ctr->queue[0], &slot);
-        if (item >= total)
-            break;
-        const uint32_t k = find_lattice(blk_prefix, n, item);
-        BatchLat *L = lats + active[k];
-        if (L->sweeps_left == 0)
-            continue;
-        const Geo g = L->g;
-        const uint32_t blk = item - blk_prefix[k];
-        assign_block_any<W>(g, blk % g.nbx, blk / g.nbx, L->spins, L->labels, L->rng_state, L->rng_sel, L->rng_iter,
-                            L->thr, L->edge, smem);
-        __syncthreads();
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        ctr->queue[3] = 0;  // measure of the previous round is finished
+    const uint32_t total = ctr->total_blocks;
+    uint2 d = load_item(items, blockIdx.x, total);
+    for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
+        const uint2 next = load_item(items, item + gridDim.x, total);
+        const BatchLat *L = lats + d.x;
+        if (L->sweeps_left != 0) {
+            const Geo g = L->g;
+            assign_block_any<W>(g, d.y & 0xFFFFu, d.y >> 16, L->spins, L->labels, L->rng_state, L->rng_sel,
+                                L->rng_iter, L->thr, L->edge, smem);
+            __syncthreads();
+        }
+        d = next;
     }
 }
 
-__global__ void __launch_bounds__(kMergeThreads) kb_merge(BatchLat *lats, const uint32_t *active, const uint32_t *blk_prefix,
-                                                          BatchCounters *ctr, unsigned int *fault)
+__global__ void __launch_bounds__(kMergeThreads) kb_merge(BatchLat *lats, const uint2 *items, BatchCounters *ctr,
+                                                          unsigned int *fault)
 {
-    __shared__ uint32_t slot;
-    if (blockIdx.x == 0 && threadIdx.x == 0)
-        ctr->queue[0] = 0;
-    const uint32_t n = ctr->n_active, total = ctr->total_blocks;
-    while (true) {
-        const uint32_t item = next_item(&ctr->queue[1], &slot);
-        if (item >= total)
-            break;
-        const uint32_t k = find_lattice(blk_prefix, n, item);
-        BatchLat *L = lats + active[k];
-        if (L->sweeps_left == 0)
-            continue;
-        const Geo g = L->g;
-        if (threadIdx.x < g.BX + g.BY)
-            merge_block(g, item - blk_prefix[k], threadIdx.x, L->edge, L->labels, fault);
+    const uint32_t total = ctr->total_blocks;
+    uint2 d = load_item(items, blockIdx.x, total);
+    for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
+        const uint2 next = load_item(items, item + gridDim.x, total);
+        const BatchLat *L = lats + d.x;
+        if (L->sweeps_left != 0) {
+            const Geo g = L->g;
+            if (threadIdx.x < g.BX + g.BY)
+                merge_block(g, (d.y >> 16) * g.nbx + (d.y & 0xFFFFu), threadIdx.x, L->edge, L->labels, fault);
+        }
+        d = next;
     }
 }
 
 // Resolve + flip of one block (flip_block); the last block of a lattice closes its round
 // (sweep count and budget).
-__global__ void __launch_bounds__(kFlipThreads, 6) kb_flip(BatchLat *lats, const uint32_t *active, const uint32_t *blk_prefix,
-                                                         BatchCounters *ctr, unsigned int *fault)
+__global__ void __launch_bounds__(kFlipThreads, 6) kb_flip(BatchLat *lats, const uint2 *items, BatchCounters *ctr,
+                                                            unsigned int *fault)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ uint32_t slot;
-    if (blockIdx.x == 0 && threadIdx.x == 0)
-        ctr->queue[1] = 0;
-    const uint32_t n = ctr->n_active, total = ctr->total_blocks;
-    while (true) {
-        const uint32_t item = next_item(&ctr->queue[2], &slot);
-        if (item >= total)
-            break;
-        const uint32_t k = find_lattice(blk_prefix, n, item);
-        BatchLat *L = lats + active[k];
-        if (L->sweeps_left == 0)
-            continue;
-        const Geo g = L->g;
-        const uint32_t blk = item - blk_prefix[k];
-        flip_block<false, 4>(g, blk % g.nbx, blk / g.nbx, L->spins, L->labels, fault, smem);
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            __threadfence();
-            if (atomicSub(&L->blocks_left, 1u) == 1u) {
-                L->blocks_left = g.nbx * g.nby;
-                L->swept = 1;
-                L->sweeps_done += 1;
-                if (L->sweeps_left != kUnlimited)
-                    L->sweeps_left -= 1;
+    const uint32_t total = ctr->total_blocks;
+    uint2 d = load_item(items, blockIdx.x, total);
+    for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
+        const uint2 next = load_item(items, item + gridDim.x, total);
+        BatchLat *L = lats + d.x;
+        if (L->sweeps_left != 0) {
+            const Geo g = L->g;
+            flip_block<false, 4>(g, d.y & 0xFFFFu, d.y >> 16, L->spins, L->labels, fault, smem);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                __threadfence();
+                if (atomicSub(&L->blocks_left, 1u) == 1u) {
+                    L->blocks_left = g.nbx * g.nby;
+                    L->swept = 1;
+                    L->sweeps_done += 1;
+                    if (L->sweeps_left != kUnlimited)
+                        L->sweeps_left -= 1;
+                }
             }
         }
+        d = next;
     }
 }
 
@@ -277,6 +269,33 @@ __global__ void kb_rng_init(const uint32_t n_tiles, const uint32_t seed_base, ui
     iter[t] = 0;
 }
 
+// One lattice's spins and its slice of the contiguous staging buffer (host transfers).
+struct StageCopy {
+    uint8_t *spins;
+    unsigned long long offset;  // byte offset in the staging buffer
+    unsigned long long bytes;
+};
+
+// Staging buffer -> lattice spins (to_lattice != 0) or back, one CTA per lattice; 16-byte
+// moves when both ends and the length allow, else 4-byte or single-byte moves.
+__global__ void kb_stage_copy(const StageCopy *c, uint8_t *stage, const int to_lattice)
+{
+    const StageCopy d = c[blockIdx.x];
+    uint8_t *a = to_lattice ? d.spins : stage + d.offset;
+    const uint8_t *s = to_lattice ? stage + d.offset : d.spins;
+    const uintptr_t align = (uintptr_t)a | (uintptr_t)s | (uintptr_t)d.bytes;
+    if ((align & 15u) == 0) {
+        for (size_t i = threadIdx.x; i < d.bytes / 16; i += blockDim.x)
+            reinterpret_cast<uint4 *>(a)[i] = reinterpret_cast<const uint4 *>(s)[i];
+    } else if ((align & 3u) == 0) {
+        for (size_t i = threadIdx.x; i < d.bytes / 4; i += blockDim.x)
+            reinterpret_cast<uint32_t *>(a)[i] = reinterpret_cast<const uint32_t *>(s)[i];
+    } else {
+        for (size_t i = threadIdx.x; i < d.bytes; i += blockDim.x)
+            a[i] = s[i];
+    }
+}
+
 __global__ void kb_hot_start(const size_t n, const uint32_t seed, uint8_t *spins)
 {
     constexpr uint32_t kChunk = 64;
@@ -316,8 +335,13 @@ struct swb_batch {
     std::vector<HostLat> lats;
     BatchLat *d_lats = nullptr;
     uint32_t *d_active = nullptr, *d_blk_prefix = nullptr, *d_chunk_prefix = nullptr;
+    uint2 *d_items = nullptr;       // flat block list (lattice slot, byi << 16 | bxi)
+    uint32_t items_cap = 0;
     BatchCounters *d_ctr = nullptr;
     unsigned int *d_fault = nullptr;
+    uint8_t *d_stage = nullptr;          // contiguous spins of update_host's lattices
+    StageCopy *d_copies = nullptr;
+    uint64_t stage_cap = 0, copies_cap = 0;
     std::vector<uint32_t> active;   // ids in the work lists
     bool lists_dirty = true;
     int grid_assign = 0, grid_other = 0, grid_merge = 0, grid_flip = 0;
@@ -383,11 +407,35 @@ int rebuild_lists(swb_batch *b)
         bp[k + 1] = bp[k] + g.nbx * g.nby;
         cp[k + 1] = cp[k] + lattice_chunks(g);
     }
+    std::vector<uint2> items;
+    items.reserve(bp[n]);
+    for (uint32_t k = 0; k < n; ++k) {
+        const Geo &g = b->lats[b->active[k]].d.g;
+        for (uint32_t by = 0; by < g.nby; ++by)
+            for (uint32_t bx = 0; bx < g.nbx; ++bx)
+                items.push_back(make_uint2(b->active[k], by << 16 | bx));
+    }
+    if (items.size() > b->items_cap) {
+        // a larger list: the captured graphs hold the old pointer
+        SWB_CUDA(cudaStreamSynchronize(b->stream));
+        for (auto &ge : b->graph)
+            if (ge) {
+                cudaGraphExecDestroy(ge);
+                ge = nullptr;
+            }
+        SWB_CUDA(cudaFree(b->d_items));
+        b->d_items = nullptr;
+        const uint32_t cap = std::max<uint32_t>((uint32_t)items.size(), 2 * b->items_cap);
+        SWB_CUDA(cudaMalloc(&b->d_items, sizeof(uint2) * cap));
+        b->items_cap = cap;
+    }
     BatchCounters c{};
     c.n_active = n;
     c.total_blocks = bp[n];
     c.total_chunks = cp[n];
     if (n) {
+        SWB_CUDA(cudaMemcpyAsync(b->d_items, items.data(), sizeof(uint2) * items.size(), cudaMemcpyHostToDevice,
+                                 b->stream));
         SWB_CUDA(cudaMemcpyAsync(b->d_active, b->active.data(), n * 4, cudaMemcpyHostToDevice, b->stream));
         SWB_CUDA(cudaMemcpyAsync(b->d_blk_prefix, bp.data(), (n + 1) * 4, cudaMemcpyHostToDevice, b->stream));
         SWB_CUDA(cudaMemcpyAsync(b->d_chunk_prefix, cp.data(), (n + 1) * 4, cudaMemcpyHostToDevice, b->stream));
@@ -397,36 +445,48 @@ int rebuild_lists(swb_batch *b)
     return SWB_OK;
 }
 
-template <int W>
-int launch_round_w(swb_batch *b, bool measure)
+int launch_assign_b(swb_batch *b)
+{
+    switch (b->W) {
+    case 8: kb_assign<8><<<b->grid_assign, kBatchThreads, b->smem_assign, b->stream>>>(b->d_lats, b->d_items, b->d_ctr); break;
+    case 16: kb_assign<16><<<b->grid_assign, kBatchThreads, b->smem_assign, b->stream>>>(b->d_lats, b->d_items, b->d_ctr); break;
+    case 32: kb_assign<32><<<b->grid_assign, kBatchThreads, b->smem_assign, b->stream>>>(b->d_lats, b->d_items, b->d_ctr); break;
+    default: return fail(SWB_ERR_ARGUMENT, "unsupported lcg width %u", b->W);
+    }
+    SWB_LAUNCHED();
+    return SWB_OK;
+}
+
+int launch_merge_b(swb_batch *b)
+{
+    kb_merge<<<b->grid_merge, kMergeThreads, 0, b->stream>>>(b->d_lats, b->d_items, b->d_ctr, b->d_fault);
+    SWB_LAUNCHED();
+    return SWB_OK;
+}
+
+int launch_flip_b(swb_batch *b)
+{
+    kb_flip<<<b->grid_flip, kFlipThreads, b->smem_flip, b->stream>>>(b->d_lats, b->d_items, b->d_ctr, b->d_fault);
+    SWB_LAUNCHED();
+    return SWB_OK;
+}
+
+int launch_round(swb_batch *b, bool measure)
 {
     kb_begin_round<<<4, 128, 0, b->stream>>>(b->d_lats, b->d_active, b->d_ctr);
     SWB_LAUNCHED();
-    kb_assign<W><<<b->grid_assign, kBatchThreads, b->smem_assign, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix,
-                                                                              b->d_ctr);
-    SWB_LAUNCHED();
-    kb_merge<<<b->grid_merge, kMergeThreads, 0, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix, b->d_ctr,
-                                                             b->d_fault);
-    SWB_LAUNCHED();
-    kb_flip<<<b->grid_flip, kFlipThreads, b->smem_flip, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix, b->d_ctr,
-                                                                      b->d_fault);
-    SWB_LAUNCHED();
+    if (int rc = launch_assign_b(b))
+        return rc;
+    if (int rc = launch_merge_b(b))
+        return rc;
+    if (int rc = launch_flip_b(b))
+        return rc;
     if (measure) {
         kb_measure<<<b->grid_other, kBatchThreads, 0, b->stream>>>(b->d_lats, b->d_active, b->d_chunk_prefix,
                                                                    b->d_ctr);
         SWB_LAUNCHED();
     }
     return SWB_OK;
-}
-
-int launch_round(swb_batch *b, bool measure)
-{
-    switch (b->W) {
-    case 8: return launch_round_w<8>(b, measure);
-    case 16: return launch_round_w<16>(b, measure);
-    case 32: return launch_round_w<32>(b, measure);
-    }
-    return fail(SWB_ERR_ARGUMENT, "unsupported lcg width %u", b->W);
 }
 
 // One round captured once per handle; it stays valid because every kernel reads the
@@ -567,6 +627,9 @@ int swb_batch_destroy(swb_batch *b)
     cudaFree(b->d_active);
     cudaFree(b->d_blk_prefix);
     cudaFree(b->d_chunk_prefix);
+    cudaFree(b->d_items);
+    cudaFree(b->d_stage);
+    cudaFree(b->d_copies);
     cudaFree(b->d_ctr);
     cudaFree(b->d_fault);
     if (b->stream)
@@ -806,20 +869,14 @@ int swb_batch_sweep_timed(swb_batch *b, uint32_t n_rounds, int per_kernel, float
             kb_begin_round<<<4, 128, 0, b->stream>>>(b->d_lats, b->d_active, b->d_ctr);
             SWB_LAUNCHED();
             SWB_CUDA(cudaEventRecord(ev[1], b->stream));
-            switch (b->W) {
-            case 8: kb_assign<8><<<b->grid_assign, kBatchThreads, b->smem_assign, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix, b->d_ctr); break;
-            case 16: kb_assign<16><<<b->grid_assign, kBatchThreads, b->smem_assign, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix, b->d_ctr); break;
-            default: kb_assign<32><<<b->grid_assign, kBatchThreads, b->smem_assign, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix, b->d_ctr); break;
-            }
-            SWB_LAUNCHED();
+            if ((rc = launch_assign_b(b)))
+                break;
             SWB_CUDA(cudaEventRecord(ev[2], b->stream));
-            kb_merge<<<b->grid_merge, kMergeThreads, 0, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix, b->d_ctr,
-                                                                     b->d_fault);
-            SWB_LAUNCHED();
+            if ((rc = launch_merge_b(b)))
+                break;
             SWB_CUDA(cudaEventRecord(ev[3], b->stream));
-            kb_flip<<<b->grid_flip, kFlipThreads, b->smem_flip, b->stream>>>(b->d_lats, b->d_active, b->d_blk_prefix,
-                                                                              b->d_ctr, b->d_fault);
-            SWB_LAUNCHED();
+            if ((rc = launch_flip_b(b)))
+                break;
             SWB_CUDA(cudaEventRecord(ev[4], b->stream));
             SWB_CUDA(cudaEventSynchronize(ev[4]));
             float t;
@@ -921,19 +978,70 @@ int swb_batch_update_host(swb_batch *b, uint32_t count, const uint32_t *ids, con
         return fail(SWB_ERR_ARGUMENT, "NULL argument");
     if (int rc = bset_device(b))
         return rc;
+    // The lattices' spins travel through one contiguous device staging buffer: host buffers
+    // that follow each other in memory move in one copy per direction, and one kernel moves
+    // the staged spins to and from the lattices.
+    std::vector<StageCopy> copies(count);
+    std::vector<bool> listed(b->capacity, false);
+    uint64_t total = 0;
     for (uint32_t k = 0; k < count; ++k) {
         HostLat *h = get_lat(b, ids[k]);
         if (!h)
             return fail(SWB_ERR_ARGUMENT, "no lattice %u", ids[k]);
-        SWB_CUDA(cudaMemcpyAsync(h->d.spins, spins_in[k], (size_t)h->d.g.L0 * h->d.g.L1, cudaMemcpyHostToDevice,
-                                 b->stream));
+        if (listed[ids[k]])
+            return fail(SWB_ERR_ARGUMENT, "lattice %u listed twice", ids[k]);
+        listed[ids[k]] = true;
+        copies[k].spins = h->d.spins;
+        copies[k].offset = total;
+        copies[k].bytes = (uint64_t)h->d.g.L0 * h->d.g.L1;
+        total += copies[k].bytes;
     }
+    if (count == 0) {
+        if (int rc = rounds(b, 1, false))
+            return rc;
+        SWB_CUDA(cudaStreamSynchronize(b->stream));
+        return SWB_OK;
+    }
+    if (total > b->stage_cap || count > b->copies_cap) {
+        SWB_CUDA(cudaStreamSynchronize(b->stream));
+        if (total > b->stage_cap) {
+            SWB_CUDA(cudaFree(b->d_stage));
+            b->d_stage = nullptr;
+            SWB_CUDA(cudaMalloc(&b->d_stage, total));
+            b->stage_cap = total;
+        }
+        if (count > b->copies_cap) {
+            SWB_CUDA(cudaFree(b->d_copies));
+            b->d_copies = nullptr;
+            SWB_CUDA(cudaMalloc(&b->d_copies, sizeof(StageCopy) * count));
+            b->copies_cap = count;
+        }
+    }
+    SWB_CUDA(cudaMemcpyAsync(b->d_copies, copies.data(), sizeof(StageCopy) * count, cudaMemcpyHostToDevice, b->stream));
+    // Runs of host buffers that are adjacent in memory, one copy each.
+    for (uint32_t k = 0; k < count;) {
+        uint32_t j = k + 1;
+        while (j < count && spins_in[j] == spins_in[j - 1] + copies[j - 1].bytes)
+            ++j;
+        SWB_CUDA(cudaMemcpyAsync(b->d_stage + copies[k].offset, spins_in[k],
+                                 copies[j - 1].offset + copies[j - 1].bytes - copies[k].offset, cudaMemcpyHostToDevice,
+                                 b->stream));
+        k = j;
+    }
+    kb_stage_copy<<<count, 512, 0, b->stream>>>(b->d_copies, b->d_stage, 1);
+    SWB_LAUNCHED();
     if (int rc = rounds(b, 1, false))
         return rc;
-    for (uint32_t k = 0; k < count; ++k) {
-        HostLat *h = get_lat(b, ids[k]);
-        SWB_CUDA(cudaMemcpyAsync(spins_out[k], h->d.spins, (size_t)h->d.g.L0 * h->d.g.L1, cudaMemcpyDeviceToHost,
+    kb_stage_copy<<<count, 512, 0, b->stream>>>(b->d_copies, b->d_stage, 0);
+    SWB_LAUNCHED();
+    for (uint32_t k = 0; k < count;) {
+        uint32_t j = k + 1;
+        while (j < count && spins_out[j] == spins_out[j - 1] + copies[j - 1].bytes)
+            ++j;
+        SWB_CUDA(cudaMemcpyAsync(spins_out[k], b->d_stage + copies[k].offset,
+                                 copies[j - 1].offset + copies[j - 1].bytes - copies[k].offset, cudaMemcpyDeviceToHost,
                                  b->stream));
+        k = j;
     }
     SWB_CUDA(cudaStreamSynchronize(b->stream));
     return SWB_OK;

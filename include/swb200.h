@@ -225,7 +225,10 @@ int swb_batch_info(swb_batch *b, uint32_t id, uint32_t *geometry);
 int swb_batch_memory(swb_batch *b, uint64_t *used, uint64_t *budget);
 
 /* One round through HOST spin buffers: copy spins_in[k] to lattice ids[k], sweep every
- * lattice once, copy the spins back to spins_out[k].  Synchronous. */
+ * lattice once, copy the spins back to spins_out[k].  Buffers that follow each other in host
+ * memory (spins_in[k + 1] == spins_in[k] + L0 * L1 of lattice ids[k]; same for spins_out) move
+ * in one copy, so one pinned arena for all lattices needs one copy per direction.  Each id at
+ * most once.  Synchronous. */
 int swb_batch_update_host(swb_batch *b, uint32_t count, const uint32_t *ids, const uint8_t *const *spins_in,
                           uint8_t *const *spins_out);
 

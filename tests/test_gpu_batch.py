@@ -135,3 +135,27 @@ def test_update_host(gpu, oracle):
     for x, o, (tile, T, seed) in zip(ins, outs, [((16, 8), 2.2, 1), ((8, 8), 2.5, 2)]):
         want, _ = _oracle_run(oracle, x, tile, T, seed, 1)
         assert np.array_equal(o, want)
+
+
+def test_update_host_contiguous_arena(gpu, oracle):
+    """Host buffers that are consecutive slices of one arena (one copy per direction) give the
+    same spins as the oracle, for lattices of different sizes; a repeated id is rejected."""
+    shapes = [((64, 64), (16, 8), 2.2, 1), ((96, 128), (8, 8), 2.5, 2), ((34, 30), (16, 4), 2.3, 3)]
+    with gpu.BatchedSW(capacity=4) as b:
+        ids = [b.add(L0, L1, T, seed, tile) for (L0, L1), tile, T, seed in shapes]
+        total = sum(L0 * L1 for (L0, L1), _, _, _ in shapes)
+        arena_in = gpu.pinned_empty((total,), np.uint8)
+        arena_out = gpu.pinned_empty((total,), np.uint8)
+        ins, outs, off = [], [], 0
+        for (L0, L1), _, _, _ in shapes:
+            x = arena_in[off:off + L0 * L1].reshape(L1, L0)
+            x[:] = oracle.hot_start(L0, L1, 1)
+            ins.append(x)
+            outs.append(arena_out[off:off + L0 * L1].reshape(L1, L0))
+            off += L0 * L1
+        b.update_host(ids, ins, outs)
+        for x, o, (_, tile, T, seed) in zip(ins, outs, shapes):
+            want, _ = _oracle_run(oracle, np.array(x), tile, T, seed, 1)
+            assert np.array_equal(o, want)
+        with pytest.raises(gpu.NativeError):
+            b.update_host([ids[0], ids[0]], [ins[0], ins[0]], [outs[0], outs[0]])
