@@ -1,14 +1,13 @@
 // Batched Swendsen-Wang: hundreds of independent periodic lattices of different sizes,
-// tiles and temperatures advance together, one persistent kernel per sweep phase.
+// tiles and temperatures advance together, one kernel launch per sweep phase for all of them.
 //
 // Work items.  Every active lattice contributes its blocks (TBX x TBY tiles) to one flat list
-// of block items (lattice slot, block coordinates), big lattices first.  The persistent CTAs
-// of kb_assign / kb_merge / kb_flip take items blockIdx.x, blockIdx.x + gridDim.x, ... and
-// load the next item's descriptor while they work on the current one; kb_measure pulls chunks
-// of 4096 sites from a device counter (atomicAdd), which kb_assign resets.  A sweep needs no
-// host work and is one CUDA graph, captured once per handle and replayed: the graph reads the
-// item totals from device memory, so adding or removing lattices does not invalidate it (only
-// growing the item list past its allocation does, which re-captures).
+// of block items (lattice slot, block coordinates), big lattices first.  kb_assign / kb_merge
+// / kb_flip run one CTA per item (a CTA takes items blockIdx.x, blockIdx.x + gridDim.x, ...,
+// loading the next item's descriptor while it works on the current one, so a smaller grid
+// also covers the list); kb_measure pulls chunks of 4096 sites from a device counter
+// (atomicAdd), which kb_assign resets.  A sweep needs no host work and is one CUDA graph,
+// captured once and replayed; it is captured again when the item count (its grid) changes.
 //
 // Per lattice the device keeps spins, labels, lcg32 streams (one per tile, seeded
 // seed_base + tile id as the reference's CPU path with one stream per tile), a sweep budget
@@ -27,7 +26,7 @@
 
 namespace swb {
 
-constexpr uint32_t kBatchThreads = 512;        // CTA size of the persistent assign and measure kernels
+constexpr uint32_t kBatchThreads = 512;        // CTA size of the assign and measure kernels
 constexpr uint32_t kMergeThreads = 192;        // merge: one thread per block edge site (BX + BY <= 160)
 constexpr uint32_t kFlipThreads = 256;         // flip: four quads of a 128 x 32 block per thread
 constexpr uint32_t kChunkSites = 4096;         // measure work item
@@ -337,6 +336,8 @@ struct swb_batch {
     uint32_t *d_active = nullptr, *d_blk_prefix = nullptr, *d_chunk_prefix = nullptr;
     uint2 *d_items = nullptr;       // flat block list (lattice slot, byi << 16 | bxi)
     uint32_t items_cap = 0;
+    uint32_t items_n = 0;           // block items in the list (the phase kernels' grid)
+    uint32_t graph_items = 0;       // items_n the captured graphs were built for
     BatchCounters *d_ctr = nullptr;
     unsigned int *d_fault = nullptr;
     uint8_t *d_stage = nullptr;          // contiguous spins of update_host's lattices
@@ -344,7 +345,7 @@ struct swb_batch {
     uint64_t stage_cap = 0, copies_cap = 0;
     std::vector<uint32_t> active;   // ids in the work lists
     bool lists_dirty = true;
-    int grid_assign = 0, grid_other = 0, grid_merge = 0, grid_flip = 0;
+    int grid_other = 0;
     uint32_t smem_assign = 0, smem_flip = 0;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};   // [measure?]
     uint64_t series_cap = 1u << 16;
@@ -429,6 +430,7 @@ int rebuild_lists(swb_batch *b)
         SWB_CUDA(cudaMalloc(&b->d_items, sizeof(uint2) * cap));
         b->items_cap = cap;
     }
+    b->items_n = (uint32_t)items.size();
     BatchCounters c{};
     c.n_active = n;
     c.total_blocks = bp[n];
@@ -445,12 +447,15 @@ int rebuild_lists(swb_batch *b)
     return SWB_OK;
 }
 
+// One CTA per block item (at least one CTA): the hardware scheduler interleaves the phases of
+// co-resident CTAs better than a persistent loop does.
 int launch_assign_b(swb_batch *b)
 {
+    const uint32_t grid = std::max(b->items_n, 1u);
     switch (b->W) {
-    case 8: kb_assign<8><<<b->grid_assign, kBatchThreads, b->smem_assign, b->stream>>>(b->d_lats, b->d_items, b->d_ctr); break;
-    case 16: kb_assign<16><<<b->grid_assign, kBatchThreads, b->smem_assign, b->stream>>>(b->d_lats, b->d_items, b->d_ctr); break;
-    case 32: kb_assign<32><<<b->grid_assign, kBatchThreads, b->smem_assign, b->stream>>>(b->d_lats, b->d_items, b->d_ctr); break;
+    case 8: kb_assign<8><<<grid, kBatchThreads, b->smem_assign, b->stream>>>(b->d_lats, b->d_items, b->d_ctr); break;
+    case 16: kb_assign<16><<<grid, kBatchThreads, b->smem_assign, b->stream>>>(b->d_lats, b->d_items, b->d_ctr); break;
+    case 32: kb_assign<32><<<grid, kBatchThreads, b->smem_assign, b->stream>>>(b->d_lats, b->d_items, b->d_ctr); break;
     default: return fail(SWB_ERR_ARGUMENT, "unsupported lcg width %u", b->W);
     }
     SWB_LAUNCHED();
@@ -459,14 +464,15 @@ int launch_assign_b(swb_batch *b)
 
 int launch_merge_b(swb_batch *b)
 {
-    kb_merge<<<b->grid_merge, kMergeThreads, 0, b->stream>>>(b->d_lats, b->d_items, b->d_ctr, b->d_fault);
+    kb_merge<<<std::max(b->items_n, 1u), kMergeThreads, 0, b->stream>>>(b->d_lats, b->d_items, b->d_ctr, b->d_fault);
     SWB_LAUNCHED();
     return SWB_OK;
 }
 
 int launch_flip_b(swb_batch *b)
 {
-    kb_flip<<<b->grid_flip, kFlipThreads, b->smem_flip, b->stream>>>(b->d_lats, b->d_items, b->d_ctr, b->d_fault);
+    kb_flip<<<std::max(b->items_n, 1u), kFlipThreads, b->smem_flip, b->stream>>>(b->d_lats, b->d_items, b->d_ctr,
+                                                                                 b->d_fault);
     SWB_LAUNCHED();
     return SWB_OK;
 }
@@ -523,6 +529,15 @@ int rounds(swb_batch *b, uint32_t n_rounds, bool any_measure)
 {
     if (int rc = rebuild_lists(b))
         return rc;
+    if (b->graph_items != b->items_n) {  // the graphs' grids follow the item count
+        SWB_CUDA(cudaStreamSynchronize(b->stream));
+        for (auto &ge : b->graph)
+            if (ge) {
+                cudaGraphExecDestroy(ge);
+                ge = nullptr;
+            }
+        b->graph_items = b->items_n;
+    }
     cudaGraphExec_t ge;
     if (int rc = round_graph(b, any_measure, &ge))
         return rc;
@@ -588,22 +603,11 @@ int swb_batch_create(swb_batch **out, uint32_t capacity, uint64_t hbm_budget_byt
     Geo gmax{};
     gmax.BX = 128; gmax.BY = 32; gmax.TBX = 32; gmax.TBY = 1; gmax.TY = 32;
     b->smem_assign = assign_smem(gmax).total;
+    b->smem_flip = flip_smem_bytes(gmax);
     int sms = 148, per_sm = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    switch (lcg_width) {
-    case 8: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kb_assign<8>, kBatchThreads, b->smem_assign); break;
-    case 16: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kb_assign<16>, kBatchThreads, b->smem_assign); break;
-    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kb_assign<32>, kBatchThreads, b->smem_assign); break;
-    }
-    b->grid_assign = sms * std::max(per_sm, 1);
-    b->smem_flip = flip_smem_bytes(gmax);
-    int per_sm2 = 1, per_sm3 = 1, per_sm4 = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, kb_merge, kMergeThreads, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm3, kb_flip, kFlipThreads, b->smem_flip);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm4, kb_measure, kBatchThreads, 0);
-    b->grid_merge = sms * std::max(per_sm2, 1);
-    b->grid_flip = sms * std::max(per_sm3, 1);
-    b->grid_other = sms * std::max(per_sm4, 1);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kb_measure, kBatchThreads, 0);
+    b->grid_other = sms * std::max(per_sm, 1);  // measure: persistent, pulls chunks
     SWB_TRY(cudaStreamSynchronize(b->stream));
 #undef SWB_TRY
     *out = b;
