@@ -601,8 +601,8 @@ int swb_batch_create(swb_batch **out, uint32_t capacity, uint64_t hbm_budget_byt
     SWB_TRY(cudaMemsetAsync(b->d_chunk_prefix, 0, 4 * (capacity + 1), b->stream));
     // The assign phase may hold any block up to 128 x 32 sites: size shared memory for it.
     Geo gmax{};
-    gmax.BX = 128; gmax.BY = 32; gmax.TBX = 32; gmax.TBY = 1; gmax.TY = 32;
-    b->smem_assign = assign_smem(gmax).total;
+    gmax.BX = 128; gmax.BY = 32;
+    b->smem_assign = assign_smem_max(lcg_width, kBatchThreads);
     b->smem_flip = flip_smem_bytes(gmax);
     int sms = 148, per_sm = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -666,7 +666,7 @@ int swb_batch_add(swb_batch *b, uint32_t L0, uint32_t L1, uint32_t tile_x, uint3
     if (slot == b->capacity)
         return fail(SWB_ERR_CAPACITY, "all %u lattice slots are in use", b->capacity);
     const Geo g = make_geo(L0, L1, tile_x, tile_y, b->W, kBatchThreads, block_x, block_y);
-    if (assign_smem(g).total > b->smem_assign)
+    if (assign_smem(g, b->W).total > b->smem_assign)
         return fail(SWB_ERR_ARGUMENT, "block of %u x %u sites needs more shared memory than reserved", g.BX, g.BY);
     const uint64_t bytes = lattice_bytes(g, b->W, b->series_cap);
     if (b->budget && b->used + bytes > b->budget)

@@ -100,25 +100,71 @@ __device__ __forceinline__ uint32_t label_global(const Geo &g, uint32_t bxi, uin
 }
 
 struct AssignSmem {
-    uint32_t parent, accM, accX, accY, edge, bond, sp, plab, total, pitch;
+    uint32_t parent, draws, slots, edge, bond, sp, plab, total, pitch;
 };
 
-__host__ __device__ inline AssignSmem assign_smem(const Geo &g)
+// Updates of every lcg32 lane in one sweep: 2 tile_y - 1 row requests of tile_x numbers and
+// the merge request of tile_x + tile_y numbers, W numbers per update.
+__host__ __device__ inline uint32_t draw_slots(const Geo &g, uint32_t W)
+{
+    return (2 * g.TY - 1) * ((g.TX + W - 1) / W) + (g.TX + g.TY + W - 1) / W;
+}
+
+__host__ __device__ inline AssignSmem assign_smem(const Geo &g, uint32_t W)
 {
     AssignSmem s{};
     const uint32_t ns = g.BX * g.BY, ntb = g.TBX * g.TBY;
     s.pitch = g.BX + 16;  // rows 16-byte aligned for cp.async
+    s.slots = draw_slots(g, W);
     s.parent = 0;
-    s.accM = s.parent + ns * 4;
-    s.accX = s.accM + ntb * 8;
-    s.accY = s.accX + ntb * g.TY * 4;
-    s.edge = s.accY + ntb * g.TY * 4;
+    s.draws = s.parent + ns * 4;                                  // [warp][slot] ballot words
+    s.edge = s.draws + ((ntb * W + 31) / 32) * s.slots * 4;
     s.bond = s.edge + kEdgeWords * 4;
     s.sp = (s.bond + ns + 15) & ~15u;
     s.plab = (s.sp + (g.BY + 1) * s.pitch + 15) & ~15u;  // uint16 provisional labels (row path)
     s.total = (s.plab + 2 * ns + 15) & ~15u;
     return s;
 }
+
+// The largest assign_smem of any tile shape with lcg width W (blocks are at most 128 x 32
+// sites, so a 128 x 32 lattice has the largest block of each shape).
+inline uint32_t assign_smem_max(uint32_t W, uint32_t max_threads)
+{
+    uint32_t m = 0;
+    for (uint32_t tx = 8; tx <= 32; tx *= 2)
+        for (uint32_t ty = 2; ty <= 32; ++ty) {
+            const uint32_t t = assign_smem(make_geo(128, 32, tx, ty, W, max_threads), W).total;
+            m = t > m ? t : m;
+        }
+    return m;
+}
+
+// Accepted draws of a block's tiles, read back from the warps' ballot words: bit k of a request
+// word is element k of the request.  Tile tb's lanes are bits (tb * W) % 32 .. + W of warp
+// (tb * W) / 32's words; a request starting at update u spans updates u .. u + ceil(n / W).
+template <int W>
+struct DrawWords {
+    const uint32_t *d;
+    uint32_t slots;
+    __device__ __forceinline__ uint32_t seg(uint32_t tb, uint32_t u) const
+    {
+        const uint32_t v = d[((tb * W) >> 5) * slots + u] >> ((tb * W) & 31);
+        return W == 32 ? v : v & ((1u << (W & 31)) - 1u);
+    }
+    // elements [0, ur * W) of the request at update u (ur * W <= 32)
+    __device__ __forceinline__ uint32_t req(uint32_t tb, uint32_t u, uint32_t ur) const
+    {
+        uint32_t v = seg(tb, u);
+        for (uint32_t s = 1; s < ur; ++s)
+            v |= seg(tb, u + s) << (s * W);
+        return v;
+    }
+    // element k of the request at update u
+    __device__ __forceinline__ uint32_t bit(uint32_t tb, uint32_t u, uint32_t k) const
+    {
+        return (seg(tb, u + k / W) >> (k % W)) & 1u;
+    }
+};
 
 // ------------------------------------------------------------------------------------------
 // kernels
@@ -150,21 +196,20 @@ __device__ __forceinline__ uint32_t spin_bits32(const uint8_t *p)
            spin_nibble(b.x) << 16 | spin_nibble(b.y) << 20 | spin_nibble(b.z) << 24 | spin_nibble(b.w) << 28;
 }
 
-// Labelling of a block whose width is a multiple of 32, from the staged spins (sp) and
-// accepted draws (accX, accY, accM) in shared memory: bond bitmasks per 32-site word, then a
-// scanline pass over x-runs (below).  The result equals the generic path's: the minimum site
-// index of each block-local component.
-template <int TXc, int TYc>
+// Labelling of a block whose width is a multiple of 32, from the staged spins (sp) and the
+// accepted draws in shared memory: bond bitmasks per 32-site word, then a scanline pass over
+// x-runs (below).  The result equals the generic path's: the minimum site index of each
+// block-local component.
+template <int W, int TXc, int TYc>
 __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uint32_t bxi, const uint32_t byi,
                                                          uint32_t *__restrict__ labels, uint32_t *__restrict__ edge,
                                                          unsigned char *smem)
 {
-    const AssignSmem L = assign_smem(g);
+    const AssignSmem L = assign_smem(g, W);
     const uint32_t TX = TXc ? TXc : g.TX, TY = TYc ? TYc : g.TY;  // compile-time for the common tiles
+    const uint32_t Ur = (TX + W - 1) / W, um = (2 * TY - 1) * Ur;  // updates per row request; merge request
     uint32_t *parent = reinterpret_cast<uint32_t *>(smem + L.parent);
-    const uint64_t *accM = reinterpret_cast<const uint64_t *>(smem + L.accM);
-    const uint32_t *accX = reinterpret_cast<const uint32_t *>(smem + L.accX);
-    const uint32_t *accY = reinterpret_cast<const uint32_t *>(smem + L.accY);
+    const DrawWords<W> dw{reinterpret_cast<const uint32_t *>(smem + L.draws), L.slots};
     uint32_t *edge_s = reinterpret_cast<uint32_t *>(smem + L.edge);
     const uint8_t *sp = smem + L.sp;
     const uint32_t BX = g.BX, BY = g.BY, NW = BX >> 5;
@@ -207,9 +252,8 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
                     const uint32_t tb = tby * g.TBX + (c0 >> txs);
                     const uint32_t iimax = min(TX, bxv - c0);
                     const uint32_t tmask = 0xFFFFFFFFu >> (32 - iimax);
-                    const uint64_t am = accM[tb];
-                    const uint32_t xb = (accX[tb * TY + jj] & (tmask >> 1)) | ((uint32_t)(am >> (TX + jj)) & 1u) << (iimax - 1);
-                    const uint32_t yb = (jj + 1 < jjmax ? accY[tb * TY + jj] : (uint32_t)am) & tmask;
+                    const uint32_t xb = (dw.req(tb, jj * Ur, Ur) & (tmask >> 1)) | dw.bit(tb, um, TX + jj) << (iimax - 1);
+                    const uint32_t yb = dw.req(tb, jj + 1 < jjmax ? (jjmax + jj) * Ur : um, Ur) & tmask;
                     AX |= xb << (k << txs);
                     AY |= yb << (k << txs);
                 }
@@ -309,7 +353,7 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
 }
 
 // Block (bxi, byi) of a lattice: lcg32 draws, bonds, union-find in shared memory.  Runs on
-// all threads of the CTA (at least TBX * TBY * W of them); smem holds assign_smem(g).total bytes.
+// all threads of the CTA (at least TBX * TBY * W of them); smem holds assign_smem(g, W).total bytes.
 template <int W, int TXc = 0, int TYc = 0>
 __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, const uint32_t byi,
                                              const uint8_t *__restrict__ spins, uint32_t *__restrict__ labels,
@@ -318,12 +362,9 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
                                              uint32_t *__restrict__ edge, uint8_t *__restrict__ dbg_bonds,
                                              uint32_t *__restrict__ dbg_assign, unsigned char *smem)
 {
-    const AssignSmem L = assign_smem(g);
+    const AssignSmem L = assign_smem(g, W);
     const uint32_t TX = TXc ? TXc : g.TX, TY = TYc ? TYc : g.TY;  // compile-time for the common tiles
     uint32_t *parent = reinterpret_cast<uint32_t *>(smem + L.parent);
-    uint64_t *accM = reinterpret_cast<uint64_t *>(smem + L.accM);
-    uint32_t *accX = reinterpret_cast<uint32_t *>(smem + L.accX);
-    uint32_t *accY = reinterpret_cast<uint32_t *>(smem + L.accY);
     uint32_t *edge_s = reinterpret_cast<uint32_t *>(smem + L.edge);
     uint8_t *bond = smem + L.bond;
     uint8_t *sp = smem + L.sp;
@@ -369,13 +410,20 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
             halo = __ldg(spins + (size_t)(y0 + tid) * g.L0 + hx);
     }
 
-    // ---- 2. lcg32 draws of this sweep, one W-lane segment per tile
+    // ---- 2. lcg32 draws of this sweep, one W-lane segment per tile.  Every update's ballot of
+    // the accept bits (the whole warp's) goes to shared memory as it is, one word per warp and
+    // update; DrawWords reads a tile's requests back.  Row request r (tile_x numbers, x rows
+    // then y rows; element k is lane k % W after update k / W + 1 of the request) starts at
+    // update r * Ur, the merge request (tile_x + tile_y numbers: bottom edge, then right edge)
+    // at update (2 tile_y - 1) * Ur; a tile shorter than tile_y idles through the rows it lacks.
     {
-        const uint32_t tb = tid / W, lane = tid % W;
+        const uint32_t tb = tid / W, lane = tid % W, lane32 = tid & 31;
         const uint32_t tgx = bxi * g.TBX + tb % g.TBX, tgy = byi * g.TBY + tb / g.TBX;
         const bool on = tb < ntb && tgx < g.n0 && tgy < g.n1;
         const uint32_t tile = tgy * g.n0 + tgx;
         const uint32_t jjmax = on ? min(TY, g.L1 - tgy * TY) : 0;
+        uint32_t *draws = reinterpret_cast<uint32_t *>(smem + L.draws) + (tid >> 5) * L.slots;
+        const bool wr = lane32 == 0 && tid < ntb * W;  // one writer per warp that holds tiles
         uint32_t st = 0, sel = 0, it = 0;
         if (on) {
             st = rng_state[(size_t)tile * W + lane];
@@ -383,143 +431,86 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
             it = rng_iter[tile];
         }
         uint32_t a = lcg_param_a(sel), c = lcg_param_c(sel);
-        uint32_t to_rot = kShuffleDistance - it % kShuffleDistance;  // updates until the next rotation
-        const uint32_t Ur = (TX + W - 1) / W, Um = (TX + TY + W - 1) / W;
-        const uint32_t nrow = on ? 2 * jjmax - 1 : 0;
-        const uint32_t seg_shift = ((tid & 31) / W) * W;
-        const uint32_t seg_mask = (W == 32) ? 0xffffffffu : ((1u << (W & 31)) - 1u);
-        // One LCG32_State::Update of every lane of the tile (random/src/lcg32.cpp:162-195): on
-        // every 15th the (a, c) pairs first rotate by state[it & (W-1)] + (it odd ? 0 : 1).
-        auto advance = [&](const bool upd) {
-            const uint32_t itn = it + 1;
-            const bool rot = upd && to_rot == 1;
-            if (__any_sync(0xffffffffu, rot)) {
-                const uint32_t src = __shfl_sync(0xffffffffu, st, itn & (W - 1), W);
-                const uint32_t from = (lane + src + ((itn & 1u) ? 0u : 1u)) & (W - 1);
-                const uint32_t a2 = __shfl_sync(0xffffffffu, a, from, W);
-                const uint32_t c2 = __shfl_sync(0xffffffffu, c, from, W);
-                const uint32_t s2 = __shfl_sync(0xffffffffu, sel, from, W);
-                if (rot) {
-                    a = a2;
-                    c = c2;
-                    sel = s2;
-                }
-            }
-            if (upd) {
-                it = itn;
-                st = a * st + c;
-                to_rot = rot ? kShuffleDistance : to_rot - 1;
+        // The parameter rotation of LCG32_State::Update (random/src/lcg32.cpp:162-195): before
+        // update itn when itn is a multiple of 15, the (a, c) pairs rotate by
+        // state[itn & (W-1)] + (itn odd ? 0 : 1).
+        auto rotate = [&](const uint32_t itn, const bool rot) {
+            const uint32_t src = __shfl_sync(0xffffffffu, st, itn & (W - 1), W);
+            const uint32_t from = (lane + src + ((itn & 1u) ? 0u : 1u)) & (W - 1);
+            const uint32_t a2 = __shfl_sync(0xffffffffu, a, from, W);
+            const uint32_t c2 = __shfl_sync(0xffffffffu, c, from, W);
+            const uint32_t s2 = __shfl_sync(0xffffffffu, sel, from, W);
+            if (rot) {
+                a = a2;
+                c = c2;
+                sel = s2;
             }
         };
-        // Full-height tiles with a compile-time shape (every tile of the warp that lies on the
-        // lattice has tile_y rows): the same sequence with the update count known at every
-        // step, so nothing is predicated; lane r % W of a tile keeps request r's word in a
-        // register and stores it after the loop.  Segments of tiles off the lattice run along
-        // and store nothing.
         bool fast = false;
         if constexpr (TXc != 0 && TYc != 0) {
-            if (__all_sync(0xffffffffu, !on || jjmax == TYc)) {
-                constexpr uint32_t kReq = 2 * TYc - 1, kWpl = (kReq + W - 1) / W;
-                constexpr uint32_t kUr = (TXc + W - 1) / W, kUm = (TXc + TYc + W - 1) / W;
-                uint32_t words[kWpl];
+            constexpr uint32_t kUr = (TXc + W - 1) / W, kRows = (2 * TYc - 1) * kUr;
+            constexpr uint32_t kN = kRows + (TXc + TYc + W - 1) / W;  // updates of this sweep
+            // Full-height tiles of a compile-time shape (every tile of the warp on the lattice has
+            // tile_y rows): the update count is known at every step, nothing is predicated, and
+            // the rotating updates come from a mask (update k rotates iff (it + k + 1) % 15 == 0).
+            // Segments of tiles off the lattice run along and store nothing.
+            if (kN <= 64 && __all_sync(0xffffffffu, !on || jjmax == TYc)) {
+                uint64_t rm = 0;
+                for (uint32_t k = kShuffleDistance - 1 - it % kShuffleDistance; k < kN; k += kShuffleDistance)
+                    rm |= 1ull << k;
+                const uint64_t wm = (uint64_t)__reduce_or_sync(0xffffffffu, (uint32_t)(rm >> 32)) << 32 |
+                                    __reduce_or_sync(0xffffffffu, (uint32_t)rm);
 #pragma unroll
-                for (uint32_t k = 0; k < kWpl; ++k)
-                    words[k] = 0;
-                // Update number k + 1 of this sweep (k compile-time after unrolling).
-                auto step = [&](const uint32_t k) {
-                    const bool rot = to_rot == 1;
-                    if (__any_sync(0xffffffffu, rot)) {
-                        const uint32_t itn = it + k + 1;
-                        const uint32_t src = __shfl_sync(0xffffffffu, st, itn & (W - 1), W);
-                        const uint32_t from = (lane + src + ((itn & 1u) ? 0u : 1u)) & (W - 1);
-                        const uint32_t a2 = __shfl_sync(0xffffffffu, a, from, W);
-                        const uint32_t c2 = __shfl_sync(0xffffffffu, c, from, W);
-                        const uint32_t s2 = __shfl_sync(0xffffffffu, sel, from, W);
-                        if (rot) {
-                            a = a2;
-                            c = c2;
-                            sel = s2;
-                        }
-                    }
+                for (uint32_t k = 0; k < kN; ++k) {
+                    if ((wm >> k) & 1u)
+                        rotate(it + k + 1, (rm >> k) & 1u);
                     st = a * st + c;
-                    to_rot = rot ? kShuffleDistance : to_rot - 1;
-                };
-#pragma unroll
-                for (uint32_t req = 0; req < kReq; ++req) {
-                    uint32_t word = 0;
-#pragma unroll
-                    for (uint32_t sub = 0; sub < kUr; ++sub) {
-                        step(req * kUr + sub);
-                        const bool bit = sub * W + lane < TXc && lcg_accept(st, thr);
-                        word |= ((__ballot_sync(0xffffffffu, bit) >> seg_shift) & seg_mask) << (sub * W);
-                    }
-                    if (lane == req % W)
-                        words[req / W] = word;
+                    const uint32_t lim = k < kRows ? TXc : TXc + TYc;          // numbers in this request
+                    const uint32_t e0 = (k < kRows ? k % kUr : k - kRows) * W;  // its first element here
+                    const uint32_t word = __ballot_sync(0xffffffffu, e0 + lane < lim && lcg_accept(st, thr));
+                    if (wr)
+                        draws[k] = word;
                 }
-                uint64_t mbits = 0;
-#pragma unroll
-                for (uint32_t sub = 0; sub < kUm; ++sub) {
-                    step(kReq * kUr + sub);
-                    const bool bit = sub * W + lane < TXc + TYc && lcg_accept(st, thr);
-                    mbits |= (uint64_t)((__ballot_sync(0xffffffffu, bit) >> seg_shift) & seg_mask) << (sub * W);
-                }
-                it += kReq * kUr + kUm;
-                if (on) {
-#pragma unroll
-                    for (uint32_t k = 0; k < kWpl; ++k) {
-                        const uint32_t req = lane + k * W;
-                        if (req < TYc)
-                            accX[tb * TYc + req] = words[k];
-                        else if (req < kReq)
-                            accY[tb * TYc + req - TYc] = words[k];
-                    }
-                    rng_state[(size_t)tile * W + lane] = st;
-                    rng_sel[(size_t)tile * W + lane] = (uint8_t)sel;
-                    if (lane == 0)
-                        rng_iter[tile] = it;
-                }
-                if (lane == 0 && tb < ntb)
-                    accM[tb] = on ? mbits : 0;
+                it += kN;
                 fast = true;
             }
         }
         if (!fast) {
-        // Row requests: tile_x numbers each, x-bond rows then y-bond rows; element k is lane
-        // k % W after update k / W + 1 of the request.  The ballot gives every lane the whole
-        // word; one lane stores it.
-#pragma unroll
-        for (uint32_t req = 0; req < 2 * TY - 1; ++req) {
-            const bool upd = req < nrow;
-            uint32_t word = 0;
-#pragma unroll
-            for (uint32_t sub = 0; sub < Ur; ++sub) {
-                advance(upd);
-                const bool bit = upd && sub * W + lane < TX && lcg_accept(st, thr);
-                word |= ((__ballot_sync(0xffffffffu, bit) >> seg_shift) & seg_mask) << (sub * W);
+            const uint32_t Ur = (TX + W - 1) / W, Um = (TX + TY + W - 1) / W;
+            const uint32_t nrow = on ? 2 * jjmax - 1 : 0;
+            uint32_t to_rot = kShuffleDistance - it % kShuffleDistance;  // updates until the next rotation
+            auto advance = [&](const bool upd) {
+                const bool rot = upd && to_rot == 1;
+                if (__any_sync(0xffffffffu, rot))
+                    rotate(it + 1, rot);
+                if (upd) {
+                    it += 1;
+                    st = a * st + c;
+                    to_rot = rot ? kShuffleDistance : to_rot - 1;
+                }
+            };
+            uint32_t u = 0;
+            for (uint32_t req = 0; req < 2 * TY - 1; ++req) {
+                const bool upd = req < nrow;
+                for (uint32_t sub = 0; sub < Ur; ++sub, ++u) {
+                    advance(upd);
+                    const uint32_t word = __ballot_sync(0xffffffffu, upd && sub * W + lane < TX && lcg_accept(st, thr));
+                    if (wr)
+                        draws[u] = word;
+                }
             }
-            if (upd && lane == (req & (W - 1))) {
-                if (req < jjmax)
-                    accX[tb * TY + req] = word;
-                else
-                    accY[tb * TY + req - jjmax] = word;
+            for (uint32_t sub = 0; sub < Um; ++sub, ++u) {
+                advance(on);
+                const uint32_t word = __ballot_sync(0xffffffffu, on && sub * W + lane < TX + TY && lcg_accept(st, thr));
+                if (wr)
+                    draws[u] = word;
             }
-        }
-        // The merge request: tile_x + tile_y numbers, [0, tile_x) bottom edge, then right edge.
-        uint64_t mbits = 0;
-#pragma unroll
-        for (uint32_t sub = 0; sub < Um; ++sub) {
-            advance(on);
-            const bool bit = on && sub * W + lane < TX + TY && lcg_accept(st, thr);
-            mbits |= (uint64_t)((__ballot_sync(0xffffffffu, bit) >> seg_shift) & seg_mask) << (sub * W);
         }
         if (on) {
             rng_state[(size_t)tile * W + lane] = st;
             rng_sel[(size_t)tile * W + lane] = (uint8_t)sel;
             if (lane == 0)
                 rng_iter[tile] = it;
-        }
-        if (lane == 0 && tb < ntb)
-            accM[tb] = mbits;
         }
     }
     asm volatile("cp.async.wait_all;\n" ::: "memory");
@@ -528,12 +519,14 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
     __syncthreads();
 
     if (dbg_assign == nullptr && (BX & 31u) == 0 && (BX & (BX - 1)) == 0) {
-        assign_block_labels_rows<TXc, TYc>(g, bxi, byi, labels, edge, smem);
+        assign_block_labels_rows<W, TXc, TYc>(g, bxi, byi, labels, edge, smem);
         return;
     }
 
     // ---- 3. bonds (bit 0 +x, bit 1 +y): equal spins and an accepted draw.  The last
     // column / row of a tile bonds through the merge draw: [0, TX) bottom, [TX, TX+TY) right.
+    const uint32_t Ur = (TX + W - 1) / W, um = (2 * TY - 1) * Ur;
+    const DrawWords<W> dw{reinterpret_cast<const uint32_t *>(smem + L.draws), L.slots};
     for (uint32_t l = tid; l < NS; l += nthr) {
         const uint32_t xl = l % BX, yl = l / BX;
         uint8_t b = 0;
@@ -542,8 +535,8 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
             const uint32_t ii = xl - tbx * TX, jj = yl - tby * TY;
             const uint32_t iimax = min(TX, bxv - tbx * TX), jjmax = min(TY, byv - tby * TY);
             const uint8_t s = sp[yl * pitch + xl];
-            const uint32_t xa = (ii + 1 < iimax) ? (accX[tb * TY + jj] >> ii) : (uint32_t)(accM[tb] >> (TX + jj));
-            const uint32_t ya = (jj + 1 < jjmax) ? (accY[tb * TY + jj] >> ii) : (uint32_t)(accM[tb] >> ii);
+            const uint32_t xa = (ii + 1 < iimax) ? dw.bit(tb, jj * Ur, ii) : dw.bit(tb, um, TX + jj);
+            const uint32_t ya = (jj + 1 < jjmax) ? dw.bit(tb, (jjmax + jj) * Ur, ii) : dw.bit(tb, um, ii);
             b = (uint8_t)(((xa & 1u) && s == sp[yl * pitch + xl + 1]) | (((ya & 1u) && s == sp[(yl + 1) * pitch + xl]) << 1));
         }
         bond[l] = b;

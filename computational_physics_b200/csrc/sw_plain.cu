@@ -386,7 +386,7 @@ int swb_create(swb_lattice **out, uint32_t L0, uint32_t L1, uint32_t tile_x, uin
     h->n = (size_t)L0 * L1;
     h->n_tiles = h->g.n0 * h->g.n1;
     h->n_blocks = h->g.nbx * h->g.nby;
-    h->smem_assign = assign_smem(h->g).total;
+    h->smem_assign = assign_smem(h->g, h->W).total;
     auto cleanup = [&](int rc) {
         swb_destroy(h);
         return rc;
@@ -865,7 +865,7 @@ int swb_sweep_static(void *stream, uint32_t L0, uint32_t L1, uint32_t tile_x, ui
     h.n = (size_t)L0 * L1;
     h.n_tiles = h.g.n0 * h.g.n1;
     h.n_blocks = h.g.nbx * h.g.nby;
-    h.smem_assign = assign_smem(h.g).total;
+    h.smem_assign = assign_smem(h.g, h.W).total;
     h.smem_flip = flip_smem_bytes(h.g);
     const size_t labels_bytes = align256(h.n * sizeof(uint32_t) + 16);
     const size_t edge_bytes = align256((size_t)h.n_blocks * kEdgeWords * sizeof(uint32_t));
