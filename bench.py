@@ -174,11 +174,11 @@ def assign_bytes(n_sites: int, n_tiles: int, W: int) -> float:
 
 # DRAM traffic of one assign launch (dram__bytes_read.sum + dram__bytes_write.sum) from one ncu
 # capture of the same kernel, per site: the batched mix of 512 lattices (39,603,200 sites:
-# 66,431,744 B read + 182,641,664 B written) and one 8192 x 8192 lattice, tile 16 x 8
-# (125,124,352 B read + 275,793,152 B written).  Traffic grows with the sites swept, so other
+# 66,080,256 B read + 171,758,080 B written) and one 8192 x 8192 lattice, tile 16 x 8
+# (111,204,096 B read + 257,027,072 B written).  Traffic grows with the sites swept, so other
 # sizes scale by their site count.
-ASSIGN_TRAFFIC_PER_SITE = {"kb_assign": (66_431_744 + 182_641_664) / 39_603_200,
-                           "k_assign": (125_124_352 + 275_793_152) / 8192 ** 2}
+ASSIGN_TRAFFIC_PER_SITE = {"kb_assign": (66_080_256 + 171_758_080) / 39_603_200,
+                           "k_assign": (111_204_096 + 257_027_072) / 8192 ** 2}
 
 
 def flip_bytes(n_sites: int) -> float:
