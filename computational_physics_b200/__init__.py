@@ -20,7 +20,7 @@ import numpy as np
 
 from ._native import NativeError, lib, lib_path, native_available  # noqa: F401
 from .lattice import SwendsenWang2D, p_add, device_count, kernel_launches, pinned_empty  # noqa: F401
-from .batch import BatchedSW, lattice_bytes, UNLIMITED  # noqa: F401
+from .batch import BatchedSW, HostIO, lattice_bytes, UNLIMITED  # noqa: F401
 
-__all__ = ["SwendsenWang2D", "BatchedSW", "p_add", "device_count", "kernel_launches", "pinned_empty",
+__all__ = ["SwendsenWang2D", "BatchedSW", "HostIO", "p_add", "device_count", "kernel_launches", "pinned_empty",
            "lattice_bytes", "UNLIMITED", "NativeError", "lib", "lib_path", "native_available"]

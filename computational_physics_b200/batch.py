@@ -1,5 +1,5 @@
-"""Many lattices on one GPU: the batched Swendsen-Wang engine (persistent kernels over a
-device work queue, one CUDA graph per round) behind the swb_batch_* C ABI."""
+"""Many lattices on one GPU: the batched Swendsen-Wang engine (one launch per sweep phase over
+all lattices' blocks, one CUDA graph per round) behind the swb_batch_* C ABI."""
 from __future__ import annotations
 
 import ctypes
@@ -34,7 +34,7 @@ extra_signatures({
 
 UNLIMITED = 0xFFFFFFFF
 
-__all__ = ["BatchedSW", "lattice_bytes", "UNLIMITED"]
+__all__ = ["BatchedSW", "HostIO", "lattice_bytes", "UNLIMITED"]
 
 
 def _ptr(a):
@@ -174,3 +174,44 @@ class BatchedSW:
         pout = (ctypes.c_void_p * k)(*[s.ctypes.data for s in spins_out])
         check(self._lib.swb_batch_update_host(self._h, k, _ptr(idarr), ctypes.cast(pin, ctypes.c_void_p),
                                               ctypes.cast(pout, ctypes.c_void_p)))
+
+    def host_io(self, ids) -> "HostIO":
+        """Pinned host buffers for update_host_io: one arena per direction, a (L1, L0) view per
+        lattice of `ids`, and the pointer arrays the C ABI takes, built once."""
+        return HostIO(self, ids)
+
+    def update_host_io(self, io: "HostIO") -> None:
+        """update_host with the buffers of `io` (io.inputs in, io.outputs out), one copy per
+        direction through the arenas and no per-call pointer work in Python."""
+        check(self._lib.swb_batch_update_host(self._h, io.count, io._ids.ctypes.data, io._pin, io._pout))
+
+
+class HostIO:
+    """Host side of repeated host-buffer sweeps of a fixed set of lattices: ``inputs`` and
+    ``outputs`` are (L1, L0) uint8 views into two pinned arenas, consecutive in memory so that
+    each direction is one copy.  :meth:`swap` exchanges them, so a step's output is the next
+    step's input."""
+
+    def __init__(self, batch: BatchedSW, ids):
+        from .lattice import pinned_empty
+        self.ids = [int(i) for i in ids]
+        self.count = len(self.ids)
+        self._ids = np.asarray(self.ids, np.uint32)
+        shapes = [batch.shapes[i] for i in self.ids]
+        total = sum(a * b for a, b in shapes)
+        self._arenas = [pinned_empty((max(total, 1),), np.uint8), pinned_empty((max(total, 1),), np.uint8)]
+        views, ptrs = [[], []], [[], []]
+        for side in (0, 1):
+            off = 0
+            for rows, cols in shapes:
+                v = self._arenas[side][off:off + rows * cols].reshape(rows, cols)
+                views[side].append(v)
+                ptrs[side].append(v.ctypes.data)
+                off += rows * cols
+        self.inputs, self.outputs = views
+        self._arrs = [(ctypes.c_void_p * self.count)(*ptrs[0]), (ctypes.c_void_p * self.count)(*ptrs[1])]
+        self._pin, self._pout = (ctypes.cast(a, ctypes.c_void_p) for a in self._arrs)
+
+    def swap(self) -> None:
+        self.inputs, self.outputs = self.outputs, self.inputs
+        self._pin, self._pout = self._pout, self._pin

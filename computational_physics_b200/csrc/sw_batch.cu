@@ -90,12 +90,12 @@ __device__ __forceinline__ uint2 load_item(const uint2 *items, uint32_t k, uint3
 }
 
 template <int W>
-__global__ void __launch_bounds__(kBatchThreads, 4) kb_assign(BatchLat *lats, const uint2 *items, BatchCounters *ctr)
+__global__ void __launch_bounds__(kBatchThreads, 4) kb_assign(BatchLat *lats, const uint2 *items, const uint32_t total,
+                                                              BatchCounters *ctr)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     if (blockIdx.x == 0 && threadIdx.x == 0)
         ctr->queue[3] = 0;  // measure of the previous round is finished
-    const uint32_t total = ctr->total_blocks;
     uint2 d = load_item(items, blockIdx.x, total);
     for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
         const uint2 next = load_item(items, item + gridDim.x, total);
@@ -110,10 +110,9 @@ __global__ void __launch_bounds__(kBatchThreads, 4) kb_assign(BatchLat *lats, co
     }
 }
 
-__global__ void __launch_bounds__(kMergeThreads) kb_merge(BatchLat *lats, const uint2 *items, BatchCounters *ctr,
+__global__ void __launch_bounds__(kMergeThreads) kb_merge(BatchLat *lats, const uint2 *items, const uint32_t total,
                                                           unsigned int *fault)
 {
-    const uint32_t total = ctr->total_blocks;
     uint2 d = load_item(items, blockIdx.x, total);
     for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
         const uint2 next = load_item(items, item + gridDim.x, total);
@@ -129,11 +128,10 @@ __global__ void __launch_bounds__(kMergeThreads) kb_merge(BatchLat *lats, const 
 
 // Resolve + flip of one block (flip_block); the last block of a lattice closes its round
 // (sweep count and budget).
-__global__ void __launch_bounds__(kFlipThreads, 6) kb_flip(BatchLat *lats, const uint2 *items, BatchCounters *ctr,
+__global__ void __launch_bounds__(kFlipThreads, 6) kb_flip(BatchLat *lats, const uint2 *items, const uint32_t total,
                                                             unsigned int *fault)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    const uint32_t total = ctr->total_blocks;
     uint2 d = load_item(items, blockIdx.x, total);
     for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
         const uint2 next = load_item(items, item + gridDim.x, total);
@@ -343,6 +341,18 @@ struct swb_batch {
     uint8_t *d_stage = nullptr;          // contiguous spins of update_host's lattices
     StageCopy *d_copies = nullptr;
     uint64_t stage_cap = 0, copies_cap = 0;
+    uint2 *d_io_items = nullptr;         // update_host's block items, grouped
+    uint64_t io_items_cap = 0;
+    cudaStream_t s_in = nullptr, s_out = nullptr;  // update_host's copy streams
+    uint64_t lists_version = 0;          // bumped by every rebuild of the work lists
+    // update_host's plan for its last id list, reused while the list and the lattice set stay
+    struct IoPlan {
+        std::vector<uint32_t> ids, gs;
+        std::vector<size_t> gi;
+        std::vector<StageCopy> copies;
+        uint64_t total = 0, version = ~0ull;
+    } io;
+    std::vector<cudaEvent_t> io_events;
     std::vector<uint32_t> active;   // ids in the work lists
     bool lists_dirty = true;
     int grid_other = 0;
@@ -444,48 +454,55 @@ int rebuild_lists(swb_batch *b)
     }
     SWB_CUDA(cudaMemcpyAsync(b->d_ctr, &c, sizeof(c), cudaMemcpyHostToDevice, b->stream));
     b->lists_dirty = false;
+    b->lists_version += 1;
     return SWB_OK;
 }
 
 // One CTA per block item (at least one CTA): the hardware scheduler interleaves the phases of
-// co-resident CTAs better than a persistent loop does.
-int launch_assign_b(swb_batch *b)
+// co-resident CTAs better than a persistent loop does.  `items` / `n` is any list of block
+// items: the whole round's, or one group of update_host's pipeline.
+int launch_assign_b(swb_batch *b, const uint2 *items, uint32_t n, cudaStream_t st)
 {
-    const uint32_t grid = std::max(b->items_n, 1u);
+    const uint32_t grid = std::max(n, 1u);
     switch (b->W) {
-    case 8: kb_assign<8><<<grid, kBatchThreads, b->smem_assign, b->stream>>>(b->d_lats, b->d_items, b->d_ctr); break;
-    case 16: kb_assign<16><<<grid, kBatchThreads, b->smem_assign, b->stream>>>(b->d_lats, b->d_items, b->d_ctr); break;
-    case 32: kb_assign<32><<<grid, kBatchThreads, b->smem_assign, b->stream>>>(b->d_lats, b->d_items, b->d_ctr); break;
+    case 8: kb_assign<8><<<grid, kBatchThreads, b->smem_assign, st>>>(b->d_lats, items, n, b->d_ctr); break;
+    case 16: kb_assign<16><<<grid, kBatchThreads, b->smem_assign, st>>>(b->d_lats, items, n, b->d_ctr); break;
+    case 32: kb_assign<32><<<grid, kBatchThreads, b->smem_assign, st>>>(b->d_lats, items, n, b->d_ctr); break;
     default: return fail(SWB_ERR_ARGUMENT, "unsupported lcg width %u", b->W);
     }
     SWB_LAUNCHED();
     return SWB_OK;
 }
 
-int launch_merge_b(swb_batch *b)
+int launch_merge_b(swb_batch *b, const uint2 *items, uint32_t n, cudaStream_t st)
 {
-    kb_merge<<<std::max(b->items_n, 1u), kMergeThreads, 0, b->stream>>>(b->d_lats, b->d_items, b->d_ctr, b->d_fault);
+    kb_merge<<<std::max(n, 1u), kMergeThreads, 0, st>>>(b->d_lats, items, n, b->d_fault);
     SWB_LAUNCHED();
     return SWB_OK;
 }
 
-int launch_flip_b(swb_batch *b)
+int launch_flip_b(swb_batch *b, const uint2 *items, uint32_t n, cudaStream_t st)
 {
-    kb_flip<<<std::max(b->items_n, 1u), kFlipThreads, b->smem_flip, b->stream>>>(b->d_lats, b->d_items, b->d_ctr,
-                                                                                 b->d_fault);
+    kb_flip<<<std::max(n, 1u), kFlipThreads, b->smem_flip, st>>>(b->d_lats, items, n, b->d_fault);
     SWB_LAUNCHED();
     return SWB_OK;
+}
+
+// The three phases of one sweep over a list of block items.
+int launch_phases_b(swb_batch *b, const uint2 *items, uint32_t n, cudaStream_t st)
+{
+    if (int rc = launch_assign_b(b, items, n, st))
+        return rc;
+    if (int rc = launch_merge_b(b, items, n, st))
+        return rc;
+    return launch_flip_b(b, items, n, st);
 }
 
 int launch_round(swb_batch *b, bool measure)
 {
     kb_begin_round<<<4, 128, 0, b->stream>>>(b->d_lats, b->d_active, b->d_ctr);
     SWB_LAUNCHED();
-    if (int rc = launch_assign_b(b))
-        return rc;
-    if (int rc = launch_merge_b(b))
-        return rc;
-    if (int rc = launch_flip_b(b))
+    if (int rc = launch_phases_b(b, b->d_items, b->items_n, b->stream))
         return rc;
     if (measure) {
         kb_measure<<<b->grid_other, kBatchThreads, 0, b->stream>>>(b->d_lats, b->d_active, b->d_chunk_prefix,
@@ -634,6 +651,13 @@ int swb_batch_destroy(swb_batch *b)
     cudaFree(b->d_items);
     cudaFree(b->d_stage);
     cudaFree(b->d_copies);
+    cudaFree(b->d_io_items);
+    for (auto e : b->io_events)
+        cudaEventDestroy(e);
+    if (b->s_in)
+        cudaStreamDestroy(b->s_in);
+    if (b->s_out)
+        cudaStreamDestroy(b->s_out);
     cudaFree(b->d_ctr);
     cudaFree(b->d_fault);
     if (b->stream)
@@ -873,13 +897,13 @@ int swb_batch_sweep_timed(swb_batch *b, uint32_t n_rounds, int per_kernel, float
             kb_begin_round<<<4, 128, 0, b->stream>>>(b->d_lats, b->d_active, b->d_ctr);
             SWB_LAUNCHED();
             SWB_CUDA(cudaEventRecord(ev[1], b->stream));
-            if ((rc = launch_assign_b(b)))
+            if ((rc = launch_assign_b(b, b->d_items, b->items_n, b->stream)))
                 break;
             SWB_CUDA(cudaEventRecord(ev[2], b->stream));
-            if ((rc = launch_merge_b(b)))
+            if ((rc = launch_merge_b(b, b->d_items, b->items_n, b->stream)))
                 break;
             SWB_CUDA(cudaEventRecord(ev[3], b->stream));
-            if ((rc = launch_flip_b(b)))
+            if ((rc = launch_flip_b(b, b->d_items, b->items_n, b->stream)))
                 break;
             SWB_CUDA(cudaEventRecord(ev[4], b->stream));
             SWB_CUDA(cudaEventSynchronize(ev[4]));
@@ -982,73 +1006,165 @@ int swb_batch_update_host(swb_batch *b, uint32_t count, const uint32_t *ids, con
         return fail(SWB_ERR_ARGUMENT, "NULL argument");
     if (int rc = bset_device(b))
         return rc;
-    // The lattices' spins travel through one contiguous device staging buffer: host buffers
-    // that follow each other in memory move in one copy per direction, and one kernel moves
-    // the staged spins to and from the lattices.
-    std::vector<StageCopy> copies(count);
-    std::vector<bool> listed(b->capacity, false);
-    uint64_t total = 0;
-    for (uint32_t k = 0; k < count; ++k) {
-        HostLat *h = get_lat(b, ids[k]);
-        if (!h)
-            return fail(SWB_ERR_ARGUMENT, "no lattice %u", ids[k]);
-        if (listed[ids[k]])
-            return fail(SWB_ERR_ARGUMENT, "lattice %u listed twice", ids[k]);
-        listed[ids[k]] = true;
-        copies[k].spins = h->d.spins;
-        copies[k].offset = total;
-        copies[k].bytes = (uint64_t)h->d.g.L0 * h->d.g.L1;
-        total += copies[k].bytes;
-    }
     if (count == 0) {
         if (int rc = rounds(b, 1, false))
             return rc;
         SWB_CUDA(cudaStreamSynchronize(b->stream));
         return SWB_OK;
     }
-    if (total > b->stage_cap || count > b->copies_cap) {
-        SWB_CUDA(cudaStreamSynchronize(b->stream));
-        if (total > b->stage_cap) {
-            SWB_CUDA(cudaFree(b->d_stage));
-            b->d_stage = nullptr;
-            SWB_CUDA(cudaMalloc(&b->d_stage, total));
-            b->stage_cap = total;
-        }
-        if (count > b->copies_cap) {
-            SWB_CUDA(cudaFree(b->d_copies));
-            b->d_copies = nullptr;
-            SWB_CUDA(cudaMalloc(&b->d_copies, sizeof(StageCopy) * count));
-            b->copies_cap = count;
-        }
-    }
-    SWB_CUDA(cudaMemcpyAsync(b->d_copies, copies.data(), sizeof(StageCopy) * count, cudaMemcpyHostToDevice, b->stream));
-    // Runs of host buffers that are adjacent in memory, one copy each.
-    for (uint32_t k = 0; k < count;) {
-        uint32_t j = k + 1;
-        while (j < count && spins_in[j] == spins_in[j - 1] + copies[j - 1].bytes)
-            ++j;
-        SWB_CUDA(cudaMemcpyAsync(b->d_stage + copies[k].offset, spins_in[k],
-                                 copies[j - 1].offset + copies[j - 1].bytes - copies[k].offset, cudaMemcpyHostToDevice,
-                                 b->stream));
-        k = j;
-    }
-    kb_stage_copy<<<count, 512, 0, b->stream>>>(b->d_copies, b->d_stage, 1);
-    SWB_LAUNCHED();
-    if (int rc = rounds(b, 1, false))
+    // The listed lattices' spins travel through one contiguous device staging buffer, in
+    // groups of about equal bytes that form a pipeline: group g's host-to-device copies (one
+    // per run of host buffers that follow each other in memory) overlap the sweep of group
+    // g - 1 and the device-to-host copies of group g - 2, on three streams.  Lattices that are
+    // not listed are swept first, while the first group's spins are still on their way.
+    if (int rc = rebuild_lists(b))
         return rc;
-    kb_stage_copy<<<count, 512, 0, b->stream>>>(b->d_copies, b->d_stage, 0);
-    SWB_LAUNCHED();
-    for (uint32_t k = 0; k < count;) {
-        uint32_t j = k + 1;
-        while (j < count && spins_out[j] == spins_out[j - 1] + copies[j - 1].bytes)
-            ++j;
-        SWB_CUDA(cudaMemcpyAsync(spins_out[k], b->d_stage + copies[k].offset,
-                                 copies[j - 1].offset + copies[j - 1].bytes - copies[k].offset, cudaMemcpyDeviceToHost,
+    auto &P = b->io;
+    const bool same = P.version == b->lists_version && P.ids.size() == count &&
+                      std::equal(P.ids.begin(), P.ids.end(), ids);
+    if (!same) {
+        std::vector<bool> listed(b->capacity, false);
+        std::vector<StageCopy> copies(count);
+        uint64_t total = 0;
+        for (uint32_t k = 0; k < count; ++k) {
+            HostLat *h = get_lat(b, ids[k]);
+            if (!h)
+                return fail(SWB_ERR_ARGUMENT, "no lattice %u", ids[k]);
+            if (listed[ids[k]])
+                return fail(SWB_ERR_ARGUMENT, "lattice %u listed twice", ids[k]);
+            listed[ids[k]] = true;
+            copies[k].spins = h->d.spins;
+            copies[k].offset = total;
+            copies[k].bytes = (uint64_t)h->d.g.L0 * h->d.g.L1;
+            total += copies[k].bytes;
+        }
+        // groups [gs[g], gs[g + 1]) of listed lattices and their block items; the unlisted
+        // active lattices' items come first
+        constexpr uint32_t kGroups = 4;  // measured: 4 groups beat 8, 12 and 16 (each group costs ~35 us of dependencies)
+        const uint32_t G = std::min(count, kGroups);
+        std::vector<uint32_t> gs(G + 1, count);
+        gs[0] = 0;
+        for (uint32_t g = 1, k = 0; g < G; ++g) {
+            const uint64_t target = total * g / G;
+            while (k < count && copies[k].offset + copies[k].bytes <= target)
+                ++k;
+            gs[g] = std::min(std::max(k, gs[g - 1] + 1), count - (G - g));  // every group keeps a lattice
+        }
+        std::vector<uint2> items;
+        auto push_items = [&](uint32_t id) {
+            const Geo &g = b->lats[id].d.g;
+            for (uint32_t by = 0; by < g.nby; ++by)
+                for (uint32_t bx = 0; bx < g.nbx; ++bx)
+                    items.push_back(make_uint2(id, by << 16 | bx));
+        };
+        for (uint32_t id : b->active)
+            if (!listed[id])
+                push_items(id);
+        std::vector<size_t> gi(G + 2, 0);
+        gi[1] = items.size();
+        for (uint32_t g = 0; g < G; ++g) {
+            for (uint32_t k = gs[g]; k < gs[g + 1]; ++k)
+                push_items(ids[k]);
+            gi[g + 2] = items.size();
+        }
+        if (total > b->stage_cap || count > b->copies_cap || items.size() > b->io_items_cap) {
+            SWB_CUDA(cudaStreamSynchronize(b->stream));
+            if (total > b->stage_cap) {
+                SWB_CUDA(cudaFree(b->d_stage));
+                b->d_stage = nullptr;
+                SWB_CUDA(cudaMalloc(&b->d_stage, total));
+                b->stage_cap = total;
+            }
+            if (count > b->copies_cap) {
+                SWB_CUDA(cudaFree(b->d_copies));
+                b->d_copies = nullptr;
+                SWB_CUDA(cudaMalloc(&b->d_copies, sizeof(StageCopy) * count));
+                b->copies_cap = count;
+            }
+            if (items.size() > b->io_items_cap) {
+                SWB_CUDA(cudaFree(b->d_io_items));
+                b->d_io_items = nullptr;
+                SWB_CUDA(cudaMalloc(&b->d_io_items, sizeof(uint2) * items.size()));
+                b->io_items_cap = items.size();
+            }
+        }
+        P.version = ~0ull;  // valid again only once the uploads below are queued
+        SWB_CUDA(cudaMemcpyAsync(b->d_copies, copies.data(), sizeof(StageCopy) * count, cudaMemcpyHostToDevice,
                                  b->stream));
-        k = j;
+        SWB_CUDA(cudaMemcpyAsync(b->d_io_items, items.data(), sizeof(uint2) * items.size(), cudaMemcpyHostToDevice,
+                                 b->stream));
+        P.ids.assign(ids, ids + count);
+        P.gs = std::move(gs);
+        P.gi = std::move(gi);
+        P.copies = std::move(copies);
+        P.total = total;
+        P.version = b->lists_version;
     }
-    SWB_CUDA(cudaStreamSynchronize(b->stream));
-    return SWB_OK;
+    const uint32_t G = (uint32_t)P.gs.size() - 1;
+    const auto &gs = P.gs;
+    const auto &gi = P.gi;
+    const auto &copies = P.copies;
+    if (!b->s_in)
+        SWB_CUDA(cudaStreamCreateWithFlags(&b->s_in, cudaStreamNonBlocking));
+    if (!b->s_out)
+        SWB_CUDA(cudaStreamCreateWithFlags(&b->s_out, cudaStreamNonBlocking));
+    while (b->io_events.size() < 2 * G) {  // [g]: group g staged; [G + g]: group g swept
+        cudaEvent_t e;
+        SWB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        b->io_events.push_back(e);
+    }
+    cudaEvent_t *ev = b->io_events.data();
+    auto run = [&]() -> int {
+        kb_begin_round<<<4, 128, 0, b->stream>>>(b->d_lats, b->d_active, b->d_ctr);
+        SWB_LAUNCHED();
+        if (gi[1])
+            if (int rc = launch_phases_b(b, b->d_io_items, (uint32_t)gi[1], b->stream))
+                return rc;
+        for (uint32_t g = 0; g < G; ++g) {
+            for (uint32_t k = gs[g]; k < gs[g + 1];) {
+                uint32_t j = k + 1;
+                while (j < gs[g + 1] && spins_in[j] == spins_in[j - 1] + copies[j - 1].bytes)
+                    ++j;
+                SWB_CUDA(cudaMemcpyAsync(b->d_stage + copies[k].offset, spins_in[k],
+                                         copies[j - 1].offset + copies[j - 1].bytes - copies[k].offset,
+                                         cudaMemcpyHostToDevice, b->s_in));
+                k = j;
+            }
+            SWB_CUDA(cudaEventRecord(ev[g], b->s_in));
+        }
+        for (uint32_t g = 0; g < G; ++g) {
+            const uint32_t n = gs[g + 1] - gs[g];
+            SWB_CUDA(cudaStreamWaitEvent(b->stream, ev[g], 0));
+            kb_stage_copy<<<n, 512, 0, b->stream>>>(b->d_copies + gs[g], b->d_stage, 1);
+            SWB_LAUNCHED();
+            if (int rc = launch_phases_b(b, b->d_io_items + gi[g + 1], (uint32_t)(gi[g + 2] - gi[g + 1]), b->stream))
+                return rc;
+            kb_stage_copy<<<n, 512, 0, b->stream>>>(b->d_copies + gs[g], b->d_stage, 0);
+            SWB_LAUNCHED();
+            SWB_CUDA(cudaEventRecord(ev[G + g], b->stream));
+            SWB_CUDA(cudaStreamWaitEvent(b->s_out, ev[G + g], 0));
+            for (uint32_t k = gs[g]; k < gs[g + 1];) {
+                uint32_t j = k + 1;
+                while (j < gs[g + 1] && spins_out[j] == spins_out[j - 1] + copies[j - 1].bytes)
+                    ++j;
+                SWB_CUDA(cudaMemcpyAsync(spins_out[k], b->d_stage + copies[k].offset,
+                                         copies[j - 1].offset + copies[j - 1].bytes - copies[k].offset,
+                                         cudaMemcpyDeviceToHost, b->s_out));
+                k = j;
+            }
+        }
+        SWB_CUDA(cudaStreamSynchronize(b->s_out));
+        SWB_CUDA(cudaStreamSynchronize(b->s_in));
+        SWB_CUDA(cudaStreamSynchronize(b->stream));
+        return SWB_OK;
+    };
+    const int rc = run();
+    if (rc) {  // leave no copy in flight behind an error
+        cudaStreamSynchronize(b->s_in);
+        cudaStreamSynchronize(b->s_out);
+        cudaStreamSynchronize(b->stream);
+    }
+    return rc ? rc : bcheck_fault(b);
 }
 
 }  // extern "C"

@@ -159,3 +159,53 @@ def test_update_host_contiguous_arena(gpu, oracle):
             assert np.array_equal(o, want)
         with pytest.raises(gpu.NativeError):
             b.update_host([ids[0], ids[0]], [ins[0], ins[0]], [outs[0], outs[0]])
+
+
+def test_update_host_sweeps_unlisted_lattices(gpu, oracle):
+    """update_host sweeps every lattice once, also those whose spins it does not move."""
+    shapes = [((64, 32), (16, 8), 2.2, 5), ((96, 64), (8, 8), 2.4, 6), ((128, 128), (32, 4), 2.3, 7)]
+    with gpu.BatchedSW(capacity=4) as b:
+        ids, starts = [], []
+        for (L0, L1), tile, T, seed in shapes:
+            i = b.add(L0, L1, T, seed, tile)
+            start = oracle.hot_start(L0, L1, seed)
+            b.set_spins(i, start)
+            ids.append(i)
+            starts.append(start)
+        out = np.empty_like(starts[1])
+        b.update_host([ids[1]], [starts[1]], [out])
+        for i, start, (_, tile, T, seed) in zip(ids, starts, shapes):
+            want, _ = _oracle_run(oracle, start, tile, T, seed, 1)
+            assert np.array_equal(b.get_spins(i), want)
+        want1, _ = _oracle_run(oracle, starts[1], shapes[1][1], shapes[1][2], shapes[1][3], 1)
+        assert np.array_equal(out, want1)
+
+
+def test_host_io_steps(gpu, oracle):
+    """HostIO arenas through update_host_io, two steps with swap(): each step's output is the
+    oracle's sweep of the previous step's."""
+    shapes = [((64, 64), (16, 8), 2.2, 11), ((34, 30), (16, 4), 2.5, 12), ((128, 96), (8, 8), 2.3, 13)]
+    with gpu.BatchedSW(capacity=4) as b:
+        ids = [b.add(L0, L1, T, seed, tile) for (L0, L1), tile, T, seed in shapes]
+        io = b.host_io(ids)
+        starts = []
+        for x, ((L0, L1), _, _, seed) in zip(io.inputs, shapes):
+            x[:] = oracle.hot_start(L0, L1, seed)
+            starts.append(np.array(x))
+        for _ in range(2):
+            b.update_host_io(io)
+            io.swap()
+        for x, start, (_, tile, T, seed) in zip(io.inputs, starts, shapes):
+            want, _ = _oracle_run(oracle, start, tile, T, seed, 2)
+            assert np.array_equal(x, want)
+        # a lattice added after the plan was made: swept too (unlisted), and the plan is rebuilt
+        extra = b.add(32, 32, 2.1, 14, (16, 8))
+        start_x = oracle.hot_start(32, 32, 14)
+        b.set_spins(extra, start_x)
+        b.update_host_io(io)
+        io.swap()
+        for x, start, (_, tile, T, seed) in zip(io.inputs, starts, shapes):
+            want, _ = _oracle_run(oracle, start, tile, T, seed, 3)
+            assert np.array_equal(x, want)
+        want_x, _ = _oracle_run(oracle, start_x, (16, 8), 2.1, 14, 1)
+        assert np.array_equal(b.get_spins(extra), want_x)
