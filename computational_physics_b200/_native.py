@@ -60,6 +60,7 @@ _SIGNATURES = {
     "swb_host_alloc": ([P, ctypes.c_size_t], I32),
     "swb_host_free": ([P], I32),
     "swb_sweep_static": ([P, U32, U32, U32, U32, U32, F32, U32, P, P, P, P, I32], I32),
+    "swb_lcg32_benchmark": ([U32, U32, U32, U64, U32, P, P, P, I32], I32),
 }
 
 

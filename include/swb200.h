@@ -166,8 +166,21 @@ int swb_sweep_static(void *stream, uint32_t L0, uint32_t L1, uint32_t tile_x, ui
                      float temperature, uint32_t n_sweeps, uint8_t *spins, uint32_t *rng_state, uint8_t *rng_sel,
                      uint32_t *rng_iter, int wait);
 
-/* ---- batched lattices: many independent lattices advanced by one persistent kernel per
- * sweep phase, replayed as a CUDA graph.  No counterpart in the reference, whose
+/* ---- the lcg32 generator on its own ---------------------------------------------------- */
+
+/* Throughput kernel of lcg32, the equivalent of the reference's TestRNG --target
+ * (random/src/test_rng.cpp, random/src/test_rng_amd_gpu.cpp:44-133): n_streams streams of
+ * lcg_width lanes, stream i seeded seed_base + i (LCG32_State::Init), each advanced
+ * updates_per_stream times (a positive multiple of 64 / lcg_width); every update yields
+ * lcg_width numbers 2^-32 * (float)u in NextReal order (random/src/lcg32.cpp:214-240).
+ * report[64] receives the last 64 numbers of stream report_id (the reference's 64-number
+ * buffer), *checksum the XOR of the bit patterns of every number generated, *ms the kernel
+ * time (CUDA events, stream initialisation included).  Synchronous. */
+int swb_lcg32_benchmark(uint32_t n_streams, uint32_t lcg_width, uint32_t seed_base, uint64_t updates_per_stream,
+                        uint32_t report_id, float *report, uint32_t *checksum, float *ms, int device);
+
+/* ---- batched lattices: many independent lattices advanced by one kernel launch per sweep
+ * phase over all their blocks, replayed as a CUDA graph.  No counterpart in the reference, whose
  * Lattice<2>::Update holds one static strategy per process (ising/include/lattice.hpp:51-57);
  * every lattice still sweeps bit-identically to the single-lattice path with the same
  * extent, tile, lcg width and seeds. ------------------------------------------------------ */
