@@ -495,13 +495,52 @@ def bench_batched(args, dist: Dist, cp) -> dict:
     return res
 
 
+def bench_serving(args, dist: Dist, cp) -> None:
+    """Continuous-batching serving: Poisson job arrivals at 10, 100 and 1000 per second, L
+    log-uniform in [32, 2048] (multiples of 16), T uniform in [1.5, 3.5], sweeps log-uniform in
+    [1e3, 1e5], a fixed 32 GB HBM budget; a bounded number of jobs per rate.  Reports job latency
+    percentiles, makespan and throughput per rate, and the same jobs of the first rate served one
+    at a time on the single-lattice path as the baseline.  Prints its own JSON line (rank 0)."""
+    from computational_physics_b200 import serving
+    n_jobs = max(8, min(args.steps, 48))
+    per_rate = {}
+    work = span = 0.0
+    with ClockSampler(dist.local_rank) as clocks:
+        for k, rate in enumerate((10.0, 100.0, 1000.0)):
+            jobs = serving.poisson_jobs(rate, n_jobs, seed=20260 + k)
+            srv = serving.Server(32 << 30)
+            try:
+                srv.run(jobs, realtime=True)
+            finally:
+                srv.close()
+            s = serving.latency_summary(jobs)
+            s["rejected"] = len(srv.rejected)
+            per_rate[str(int(rate))] = s
+            work += sum(j.site_updates for j in jobs if j.done is not None)
+            span += s.get("makespan_s", 0.0)
+        base_jobs = serving.poisson_jobs(10.0, n_jobs, seed=20260)
+        serving.SequentialServer().run(base_jobs, realtime=True)
+        base = serving.latency_summary(base_jobs)
+    if dist.rank != 0:
+        return
+    print(json.dumps({
+        "metric": "SW spin-updates/s", "value": work / span, "unit": "spin-updates/s", "n_gpus": dist.world,
+        "steps": n_jobs, "warmup": 0, "ms_per_step": 1e3 * span / (3 * n_jobs), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": "serving: Poisson arrivals at 10/100/1000 per s, L log-uniform [32, 2048], "
+                               "T uniform [1.5, 3.5], sweeps log-uniform [1e3, 1e5], 32 GB HBM budget",
+                   "jobs_per_rate": n_jobs, "parallelism": f"replicas x{dist.world}"},
+        "serving": per_rate, "sequential_baseline_rate10": base, "clocks": clocks.summary(),
+    }))
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batched", choices=["batched", *PLAIN])
+    ap.add_argument("--workload", default="batched", choices=["batched", *PLAIN, "serving"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true", help="skip the plain-loop comparison and the energy gate")
     ap.add_argument("--_ref-worker", dest="ref_worker_mode", action="store_true")
@@ -519,6 +558,9 @@ def main() -> None:
         import computational_physics_b200 as cp
         if cp.device_count() < 1:
             raise RuntimeError("no CUDA device")
+        if args.workload == "serving":
+            bench_serving(args, dist, cp)
+            return
         r = bench_batched(args, dist, cp) if args.workload == "batched" else bench_plain(args, dist, cp)
         if dist.rank != 0:
             return

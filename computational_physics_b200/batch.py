@@ -27,6 +27,7 @@ extra_signatures({
     "swb_batch_accumulators": ([P, U32, P], I32),
     "swb_batch_samples": ([P, U32, P, U64, P], I32),
     "swb_batch_get_rng": ([P, U32, P, P, P, P], I32),
+    "swb_batch_set_rng": ([P, U32, P, P, P, P], I32),
     "swb_batch_info": ([P, U32, P], I32),
     "swb_batch_memory": ([P, P, P], I32),
     "swb_batch_update_host": ([P, U32, P, P, P], I32),
@@ -154,6 +155,35 @@ class BatchedSW:
         it = np.empty(nt, np.uint32)
         check(self._lib.swb_batch_get_rng(self._h, lid, _ptr(st), _ptr(a), _ptr(c), _ptr(it)))
         return st, a, c, it
+
+    def set_rng(self, lid: int, state, a, c, iteration) -> None:
+        nt, w = self.info(lid)["tiles"], self.lcg_width
+        arrs = [np.ascontiguousarray(x, np.uint32) for x in (state, a, c, iteration)]
+        if any(x.size != nt * w for x in arrs[:3]) or arrs[3].size != nt:
+            raise ValueError("rng arrays have the wrong size")
+        check(self._lib.swb_batch_set_rng(self._h, lid, *[_ptr(x) for x in arrs]))
+
+    def snapshot(self, lid: int) -> dict:
+        """Everything needed to resume lattice `lid` bit-identically elsewhere (another slot,
+        batch or process): geometry, spins, lcg32 streams, sweeps done and the recorded
+        observables.  See :mod:`computational_physics_b200.snapshot` for the file format."""
+        g = self.info(lid)
+        st, a, c, it = self.get_rng(lid)
+        return {"L0": g["L0"], "L1": g["L1"], "tile": (g["tile_x"], g["tile_y"]), "lcg_width": self.lcg_width,
+                "spins": self.get_spins(lid), "rng_state": st, "rng_a": a, "rng_c": c, "rng_iteration": it,
+                "sweeps_done": self.status(lid)[1], "samples": self.samples(lid),
+                "accumulators": self.accumulators(lid)}
+
+    def restore(self, lid: int, snap: dict) -> None:
+        """Loads a snapshot's spins and lcg32 streams into lattice `lid`, which must have the same
+        extent, tile and lcg width.  Its sweeps then continue the snapshot's Markov chain exactly;
+        the snapshot's samples and accumulators stay with the caller."""
+        g = self.info(lid)
+        if (g["L0"], g["L1"], (g["tile_x"], g["tile_y"]), self.lcg_width) != \
+                (snap["L0"], snap["L1"], tuple(snap["tile"]), snap["lcg_width"]):
+            raise ValueError("snapshot geometry does not match the lattice")
+        self.set_spins(lid, snap["spins"])
+        self.set_rng(lid, snap["rng_state"], snap["rng_a"], snap["rng_c"], snap["rng_iteration"])
 
     def info(self, lid: int) -> dict:
         v = np.zeros(8, np.uint32)

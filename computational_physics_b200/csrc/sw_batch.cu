@@ -979,6 +979,29 @@ int swb_batch_get_rng(swb_batch *b, uint32_t id, uint32_t *state, uint32_t *a, u
     return SWB_OK;
 }
 
+int swb_batch_set_rng(swb_batch *b, uint32_t id, const uint32_t *state, const uint32_t *a, const uint32_t *c,
+                      const uint32_t *iteration)
+{
+    HostLat *h = get_lat(b, id);
+    if (!h || !state || !a || !c || !iteration)
+        return fail(SWB_ERR_ARGUMENT, "no lattice %u or NULL argument", id);
+    if (int rc = bset_device(b))
+        return rc;
+    const size_t tiles = (size_t)h->d.g.n0 * h->d.g.n1, nw = tiles * b->W;
+    std::vector<uint8_t> sel(nw);
+    for (size_t i = 0; i < nw; ++i) {
+        const int k = lcg_pair_index(a[i], c[i]);
+        if (k < 0)
+            return fail(SWB_ERR_ARGUMENT, "lane %zu: (a, c) = (%u, %u) is not an lcg32 parameter pair", i, a[i], c[i]);
+        sel[i] = (uint8_t)k;
+    }
+    SWB_CUDA(cudaMemcpyAsync(h->d.rng_state, state, nw * 4, cudaMemcpyHostToDevice, b->stream));
+    SWB_CUDA(cudaMemcpyAsync(h->d.rng_sel, sel.data(), nw, cudaMemcpyHostToDevice, b->stream));
+    SWB_CUDA(cudaMemcpyAsync(h->d.rng_iter, iteration, tiles * 4, cudaMemcpyHostToDevice, b->stream));
+    SWB_CUDA(cudaStreamSynchronize(b->stream));
+    return SWB_OK;
+}
+
 int swb_batch_info(swb_batch *b, uint32_t id, uint32_t *geometry)
 {
     HostLat *h = get_lat(b, id);

@@ -22,6 +22,15 @@ __host__ __device__ __forceinline__ uint32_t lcg_param_c(uint32_t sel)
     return sel == 0 ? 1289706101u : sel == 1 ? 1640531513u : sel == 2 ? 797082193u : sel == 3 ? 626627237u : 1013904223u;
 }
 
+// Index (0..4) of an (a, c) pair among the five, or -1 (host code, for imported streams).
+inline int lcg_pair_index(uint32_t a, uint32_t c)
+{
+    for (uint32_t s = 0; s < 5; ++s)
+        if (lcg_param_a(s) == a && lcg_param_c(s) == c)
+            return (int)s;
+    return -1;
+}
+
 constexpr uint32_t kShuffleDistance = 15;          // LCG32_State::ShuffleDistance (lcg32.hpp:43)
 constexpr float kTwoPowMinus32 = 2.3283064365386963e-10f;  // the float the reference's literal rounds to
 

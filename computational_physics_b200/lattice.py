@@ -190,6 +190,22 @@ class SwendsenWang2D:
             raise ValueError("rng arrays have the wrong size")
         check(self._lib.swb_set_rng(self._h, *[_ptr(x) for x in arrs]))
 
+    def snapshot(self) -> dict:
+        """Spins, lcg32 streams and recorded observables: enough to resume this lattice
+        bit-identically in another handle or process (see :mod:`computational_physics_b200.snapshot`)."""
+        st, a, c, it = self.get_rng()
+        return {"L0": self.L0, "L1": self.L1, "tile": self.tile, "lcg_width": self.lcg_width,
+                "spins": self.get_spins(), "rng_state": st, "rng_a": a, "rng_c": c, "rng_iteration": it,
+                "samples": self.samples(), "accumulators": self.accumulators()}
+
+    def restore(self, snap: dict) -> None:
+        """Loads a snapshot's spins and lcg32 streams (same extent, tile and lcg width)."""
+        if (self.L0, self.L1, self.tile, self.lcg_width) != (snap["L0"], snap["L1"], tuple(snap["tile"]),
+                                                            snap["lcg_width"]):
+            raise ValueError("snapshot geometry does not match the lattice")
+        self.set_spins(snap["spins"])
+        self.set_rng(snap["rng_state"], snap["rng_a"], snap["rng_c"], snap["rng_iteration"])
+
     def device_buffers(self) -> tuple[int, int]:
         s = ctypes.c_void_p()
         l = ctypes.c_void_p()

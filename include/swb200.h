@@ -232,6 +232,10 @@ int swb_batch_sweep_timed(swb_batch *b, uint32_t n_rounds, int per_kernel, float
 int swb_batch_accumulators(swb_batch *b, uint32_t id, double *out);
 int swb_batch_samples(swb_batch *b, uint32_t id, int64_t *em, uint64_t capacity, uint64_t *count);
 int swb_batch_get_rng(swb_batch *b, uint32_t id, uint32_t *state, uint32_t *a, uint32_t *c, uint32_t *iteration);
+/* Imports lattice id's lcg32 streams (as swb_set_rng): with the spins, the whole state a
+ * preempted job needs to resume bit-identically.  Synchronous. */
+int swb_batch_set_rng(swb_batch *b, uint32_t id, const uint32_t *state, const uint32_t *a, const uint32_t *c,
+                      const uint32_t *iteration);
 
 /* geometry[8] = L0, L1, tile_x, tile_y, tiles per block x, tiles per block y, tiles, blocks. */
 int swb_batch_info(swb_batch *b, uint32_t id, uint32_t *geometry);

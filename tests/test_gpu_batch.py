@@ -209,3 +209,31 @@ def test_host_io_steps(gpu, oracle):
             assert np.array_equal(x, want)
         want_x, _ = _oracle_run(oracle, start_x, (16, 8), 2.1, 14, 1)
         assert np.array_equal(b.get_spins(extra), want_x)
+
+
+def test_snapshot_resume_bit_identical(gpu, tmp_path):
+    """Preempt a job (snapshot to disk), resume it in another batch and another slot, and in a
+    single-lattice handle: every continuation equals the uninterrupted run."""
+    from computational_physics_b200 import snapshot
+    with gpu.BatchedSW(capacity=4) as b:
+        b.add(48, 48, 2.4, 3, (16, 8))
+        lid = b.add(96, 64, 2.3, 9, (16, 8))
+        b.hot_start(lid, 9)
+        b.sweep(7)
+        snap = b.snapshot(lid)
+        path = str(tmp_path / "job.npz")
+        snapshot.save(path, snap)
+        b.sweep(5)
+        want = b.get_spins(lid)
+    loaded = snapshot.load(path)
+    assert loaded["sweeps_done"] == 7 and loaded["spins"].shape == (64, 96)
+    with gpu.BatchedSW(capacity=4) as b2:
+        b2.add(32, 32, 2.0, 1, (16, 8))
+        k = b2.add(96, 64, 2.3, 1234, (16, 8))     # other seed: restore replaces the streams
+        b2.restore(k, loaded)
+        b2.sweep(5)
+        assert np.array_equal(b2.get_spins(k), want)
+    with gpu.SwendsenWang2D(96, 64, (16, 8), 16, seed_base=77) as sw:
+        sw.restore(loaded)
+        sw.update(2.3, 5)
+        assert np.array_equal(sw.get_spins(), want)
