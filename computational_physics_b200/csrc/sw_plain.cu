@@ -6,17 +6,18 @@
 //
 //   k_assign  [AssignLabels + the in-block part of MergeLabels]  one CTA per block of
 //             TBX x TBY tiles.  Each tile's lcg32 stream lives in the registers of one
-//             W-lane warp segment; the bond draws become bit masks via __ballot_sync.
-//             Spins of the block plus a one-site halo are staged in shared memory, bonds
-//             are formed, and a lock-free union-find toward the minimum index labels the
-//             block in shared memory (tile-local bonds first -- the reference's
-//             AssignLabels result -- then the bonds between tiles of the block).  Writes
-//             each site's block-local minimum global index and the bond bits of the
-//             block's right and bottom edge.
+//             W-lane warp segment; the accept bits of every update are warp ballots.
+//             Spins of the block plus a one-site halo are staged in shared memory, bond
+//             words are formed bit-parallel, and a scanline pass with a lock-free union-find
+//             toward the minimum index labels the block in shared memory.  Writes each
+//             site's label (block roots: their global index; other sites: the block-local
+//             index of their root) and the bond bits of the block's right and bottom edge.
+//             A recorded sweep (kDebug) labels tile by tile first, as the reference's
+//             AssignLabels does, to dump that stage.
 //   k_merge   [MergeLabels across blocks]  atomicMin union on the global label array for
 //             the edge bonds recorded by k_assign.
-//   k_flip    [ResolveLabels + FlipClusters]  pointer chase to the root (the cluster's
-//             minimum site index) and spin ^= root & 1.
+//   k_flip    [ResolveLabels + FlipClusters]  each merged block root's chain is walked once
+//             to the root (the cluster's minimum site index); spin ^= root & 1.
 //
 // k_measure (every measure_every-th sweep) reduces energy and magnetisation on the device
 // and accumulates E, E^2, |M| in FP64 (Lattice<2>::GetEnergyAndMagnetization,
