@@ -337,14 +337,39 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
 
     // Labels: a block root stores its global site index (the merge links these), every other
     // site kLocalFlag | the block-local index of its root.
-    for (uint32_t yl = warp; yl < byv; yl += nwarps) {
-        uint32_t *row = labels + (size_t)(y0 + yl) * g.L0 + x0;
-        for (uint32_t w = 0; w < NW; ++w) {
-            const uint32_t xl = (w << 5) + lane;
-            if (xl < bxv) {
-                const uint32_t l = yl * BX + xl;
-                const uint32_t r = uf_find_halve(parent, plab[l]);
-                row[xl] = r == l ? (y0 + yl) * g.L0 + x0 + xl : (kLocalFlag | r);
+    if ((g.L0 & 3u) == 0) {
+        // four sites per thread: one 8-byte load of provisional labels, four independent finds,
+        // one 16-byte store (rows and x0 are 16-byte aligned: L0 and BX are multiples of 4)
+        const uint32_t nq = BX >> 2, qs = 31 - __clz(nq);
+        for (uint32_t i = tid; i < (byv << qs); i += blockDim.x) {
+            const uint32_t yl = i >> qs, x4 = (i & (nq - 1)) << 2;
+            if (x4 < bxv) {
+                const uint32_t l = yl * BX + x4;
+                const uint2 pp = *reinterpret_cast<const uint2 *>(plab + l);
+                const uint32_t p[4] = {pp.x & 0xFFFFu, pp.x >> 16, pp.y & 0xFFFFu, pp.y >> 16};
+                uint32_t r[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    r[k] = uf_find_halve(parent, p[k]);
+                const uint32_t gb = (y0 + yl) * g.L0 + x0 + x4;
+                uint4 o;
+                o.x = r[0] == l ? gb : (kLocalFlag | r[0]);
+                o.y = r[1] == l + 1 ? gb + 1 : (kLocalFlag | r[1]);
+                o.z = r[2] == l + 2 ? gb + 2 : (kLocalFlag | r[2]);
+                o.w = r[3] == l + 3 ? gb + 3 : (kLocalFlag | r[3]);
+                *reinterpret_cast<uint4 *>(labels + (size_t)(y0 + yl) * g.L0 + x0 + x4) = o;
+            }
+        }
+    } else {
+        for (uint32_t yl = warp; yl < byv; yl += nwarps) {
+            uint32_t *row = labels + (size_t)(y0 + yl) * g.L0 + x0;
+            for (uint32_t w = 0; w < NW; ++w) {
+                const uint32_t xl = (w << 5) + lane;
+                if (xl < bxv) {
+                    const uint32_t l = yl * BX + xl;
+                    const uint32_t r = uf_find_halve(parent, plab[l]);
+                    row[xl] = r == l ? (y0 + yl) * g.L0 + x0 + xl : (kLocalFlag | r);
+                }
             }
         }
     }
