@@ -412,23 +412,38 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
         const uint32_t warp = tid >> 5, lane32 = tid & 31, nwarps = nthr >> 5;
         const uint32_t hy = (y0 + byv) % g.L1;
         const uint32_t vec = (g.L0 % 16 == 0 && BX % 16 == 0) ? 16 : (g.L0 % 4 == 0 ? 4 : 1);
-        for (uint32_t yl = warp; yl <= byv; yl += nwarps) {
-            const uint32_t gy = yl < byv ? y0 + yl : hy;
-            const uint8_t *row = spins + (size_t)gy * g.L0 + x0;
-            uint8_t *dst = sp + yl * pitch;
-            if (vec == 16) {
-                for (uint32_t v = lane32; v * 16 < bxv; v += 32)
+        if (vec == 16 && (BX & (BX - 1)) == 0) {
+            // one 16-byte copy per thread, rows packed across the CTA (a 128-wide row is 8
+            // copies, so a warp moves 4 rows at once)
+            const uint32_t nv = BX >> 4, vs = 31 - __clz(nv);
+            for (uint32_t i = tid; i < ((byv + 1) << vs); i += nthr) {
+                const uint32_t yl = i >> vs, v = i & (nv - 1);
+                if (v * 16 < bxv) {
+                    const uint32_t gy = yl < byv ? y0 + yl : hy;
                     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(
-                                     (uint32_t)__cvta_generic_to_shared(dst + 16 * v)),
-                                 "l"(row + 16 * v));
-            } else if (vec == 4) {
-                for (uint32_t v = lane32; v * 4 < bxv; v += 32)
-                    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(
-                                     (uint32_t)__cvta_generic_to_shared(dst + 4 * v)),
-                                 "l"(row + 4 * v));
-            } else {
-                for (uint32_t x = lane32; x < bxv; x += 32)
-                    dst[x] = __ldg(row + x);
+                                     (uint32_t)__cvta_generic_to_shared(sp + yl * pitch + 16 * v)),
+                                 "l"(spins + (size_t)gy * g.L0 + x0 + 16 * v));
+                }
+            }
+        } else {
+            for (uint32_t yl = warp; yl <= byv; yl += nwarps) {
+                const uint32_t gy = yl < byv ? y0 + yl : hy;
+                const uint8_t *row = spins + (size_t)gy * g.L0 + x0;
+                uint8_t *dst = sp + yl * pitch;
+                if (vec == 16) {
+                    for (uint32_t v = lane32; v * 16 < bxv; v += 32)
+                        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(
+                                         (uint32_t)__cvta_generic_to_shared(dst + 16 * v)),
+                                     "l"(row + 16 * v));
+                } else if (vec == 4) {
+                    for (uint32_t v = lane32; v * 4 < bxv; v += 32)
+                        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(
+                                         (uint32_t)__cvta_generic_to_shared(dst + 4 * v)),
+                                     "l"(row + 4 * v));
+                } else {
+                    for (uint32_t x = lane32; x < bxv; x += 32)
+                        dst[x] = __ldg(row + x);
+                }
             }
         }
         if (tid < byv)
