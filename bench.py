@@ -172,13 +172,14 @@ def assign_bytes(n_sites: int, n_tiles: int, W: int) -> float:
     return n_sites * 5 + n_tiles * 2 * (W * 5 + 4)
 
 
-# DRAM traffic of one assign launch (dram__bytes_read.sum + dram__bytes_write.sum) from one ncu
-# capture of the same kernel, per site: the batched mix of 512 lattices (39,603,200 sites:
-# 66,080,256 B read + 171,758,080 B written) and one 8192 x 8192 lattice, tile 16 x 8
-# (111,204,096 B read + 257,027,072 B written).  Traffic grows with the sites swept, so other
-# sizes scale by their site count.
-ASSIGN_TRAFFIC_PER_SITE = {"kb_assign": (66_080_256 + 171_758_080) / 39_603_200,
-                           "k_assign": (111_204_096 + 257_027_072) / 8192 ** 2}
+# DRAM traffic of one assign pass over a workload (dram__bytes_read.sum + dram__bytes_write.sum)
+# from one ncu capture of the same kernel, per site: the batched mix of 512 lattices (39,603,200
+# sites; the round runs its two lattice groups as two launches: 33,179,392 + 33,145,344 B read,
+# 60,603,136 + 64,940,032 B written) and one 8192 x 8192 lattice, tile 16 x 8 (111,338,496 B read
+# + 253,723,904 B written).  Traffic grows with the sites swept, so other sizes scale by their
+# site count.
+ASSIGN_TRAFFIC_PER_SITE = {"kb_assign": (33_179_392 + 33_145_344 + 60_603_136 + 64_940_032) / 39_603_200,
+                           "k_assign": (111_338_496 + 253_723_904) / 8192 ** 2}
 
 
 def flip_bytes(n_sites: int) -> float:
