@@ -6,8 +6,9 @@
 // / kb_flip run one CTA per item (a CTA takes items blockIdx.x, blockIdx.x + gridDim.x, ...,
 // loading the next item's descriptor while it works on the current one, so a smaller grid
 // also covers the list); kb_measure pulls chunks of 4096 sites from a device counter
-// (atomicAdd), which kb_assign resets.  A sweep needs no host work and is one CUDA graph,
-// captured once and replayed; it is captured again when the item count (its grid) changes.
+// (atomicAdd), which kb_assign resets.  A sweep needs no host work and is one CUDA graph: the
+// lattices split into two groups whose phase kernels run on two streams side by side; the
+// graph is captured once and replayed, and captured again when the lattice set changes.
 //
 // Per lattice the device keeps spins, labels, lcg32 streams (one per tile, seeded
 // seed_base + tile id as the reference's CPU path with one stream per tile), a sweep budget
@@ -53,10 +54,9 @@ struct BatchLat {
 };
 
 struct BatchCounters {
-    unsigned int queue[4];    // assign, merge, flip, measure
-    unsigned int n_active;    // lattices in the work lists
-    unsigned int total_blocks;
-    unsigned int total_chunks;
+    unsigned int measure_next;  // next measure chunk (device work counter)
+    unsigned int n_active;      // lattices in the work lists
+    unsigned int total_chunks;  // measure chunks of all active lattices
     unsigned int pad;
 };
 
@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4) kb_assign(BatchLat *lats, co
 {
     extern __shared__ __align__(16) unsigned char smem[];
     if (blockIdx.x == 0 && threadIdx.x == 0)
-        ctr->queue[3] = 0;  // measure of the previous round is finished
+        ctr->measure_next = 0;  // measure of the previous round is finished
     uint2 d = load_item(items, blockIdx.x, total);
     for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
         const uint2 next = load_item(items, item + gridDim.x, total);
@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(kBatchThreads) kb_measure(BatchLat *lats, cons
     __shared__ long long se[kBatchThreads / 32], sm[kBatchThreads / 32];
     const uint32_t n = ctr->n_active, total = ctr->total_chunks;
     while (true) {
-        const uint32_t item = next_item(&ctr->queue[3], &slot);
+        const uint32_t item = next_item(&ctr->measure_next, &slot);
         if (item >= total)
             break;
         const uint32_t k = find_lattice(chunk_prefix, n, item);
@@ -332,7 +332,7 @@ struct swb_batch {
     uint64_t budget = 0, used = 0;
     std::vector<HostLat> lats;
     BatchLat *d_lats = nullptr;
-    uint32_t *d_active = nullptr, *d_blk_prefix = nullptr, *d_chunk_prefix = nullptr;
+    uint32_t *d_active = nullptr, *d_chunk_prefix = nullptr;
     uint2 *d_items = nullptr;       // flat block list (lattice slot, byi << 16 | bxi)
     uint32_t items_cap = 0;
     uint32_t items_n = 0;           // block items in the list (the phase kernels' grid)
@@ -359,7 +359,7 @@ struct swb_batch {
     std::vector<cudaEvent_t> io_events;
     std::vector<uint32_t> active;   // ids in the work lists
     bool lists_dirty = true;
-    int grid_other = 0;
+    int grid_measure = 0;
     uint32_t smem_assign = 0, smem_flip = 0;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};   // [measure?]
     uint64_t series_cap = 1u << 16;
@@ -465,13 +465,11 @@ int rebuild_lists(swb_batch *b)
     b->items_n = (uint32_t)items.size();
     BatchCounters c{};
     c.n_active = n;
-    c.total_blocks = bp[n];
     c.total_chunks = cp[n];
     if (n) {
         SWB_CUDA(cudaMemcpyAsync(b->d_items, items.data(), sizeof(uint2) * items.size(), cudaMemcpyHostToDevice,
                                  b->stream));
         SWB_CUDA(cudaMemcpyAsync(b->d_active, b->active.data(), n * 4, cudaMemcpyHostToDevice, b->stream));
-        SWB_CUDA(cudaMemcpyAsync(b->d_blk_prefix, bp.data(), (n + 1) * 4, cudaMemcpyHostToDevice, b->stream));
         SWB_CUDA(cudaMemcpyAsync(b->d_chunk_prefix, cp.data(), (n + 1) * 4, cudaMemcpyHostToDevice, b->stream));
     }
     SWB_CUDA(cudaMemcpyAsync(b->d_ctr, &c, sizeof(c), cudaMemcpyHostToDevice, b->stream));
@@ -545,7 +543,7 @@ int launch_round(swb_batch *b, bool measure)
         SWB_CUDA(cudaStreamWaitEvent(b->stream, b->join[q], 0));
     }
     if (measure) {
-        kb_measure<<<b->grid_other, kBatchThreads, 0, b->stream>>>(b->d_lats, b->d_active, b->d_chunk_prefix,
+        kb_measure<<<b->grid_measure, kBatchThreads, 0, b->stream>>>(b->d_lats, b->d_active, b->d_chunk_prefix,
                                                                    b->d_ctr);
         SWB_LAUNCHED();
     }
@@ -649,13 +647,11 @@ int swb_batch_create(swb_batch **out, uint32_t capacity, uint64_t hbm_budget_byt
     SWB_TRY(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     SWB_TRY(cudaMalloc(&b->d_lats, sizeof(BatchLat) * capacity));
     SWB_TRY(cudaMalloc(&b->d_active, 4 * capacity));
-    SWB_TRY(cudaMalloc(&b->d_blk_prefix, 4 * (capacity + 1)));
     SWB_TRY(cudaMalloc(&b->d_chunk_prefix, 4 * (capacity + 1)));
     SWB_TRY(cudaMalloc(&b->d_ctr, sizeof(BatchCounters)));
     SWB_TRY(cudaMalloc(&b->d_fault, sizeof(unsigned int)));
     SWB_TRY(cudaMemsetAsync(b->d_fault, 0, sizeof(unsigned int), b->stream));
     SWB_TRY(cudaMemsetAsync(b->d_ctr, 0, sizeof(BatchCounters), b->stream));
-    SWB_TRY(cudaMemsetAsync(b->d_blk_prefix, 0, 4 * (capacity + 1), b->stream));
     SWB_TRY(cudaMemsetAsync(b->d_chunk_prefix, 0, 4 * (capacity + 1), b->stream));
     // The assign phase may hold any block up to 128 x 32 sites: size shared memory for it.
     Geo gmax{};
@@ -665,7 +661,7 @@ int swb_batch_create(swb_batch **out, uint32_t capacity, uint64_t hbm_budget_byt
     int sms = 148, per_sm = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kb_measure, kBatchThreads, 0);
-    b->grid_other = sms * std::max(per_sm, 1);  // measure: persistent, pulls chunks
+    b->grid_measure = sms * std::max(per_sm, 1);  // measure: persistent, pulls chunks
     SWB_TRY(cudaStreamSynchronize(b->stream));
 #undef SWB_TRY
     *out = b;
@@ -687,7 +683,6 @@ int swb_batch_destroy(swb_batch *b)
             cudaFree(l.mem);
     cudaFree(b->d_lats);
     cudaFree(b->d_active);
-    cudaFree(b->d_blk_prefix);
     cudaFree(b->d_chunk_prefix);
     cudaFree(b->d_items);
     cudaFree(b->d_stage);

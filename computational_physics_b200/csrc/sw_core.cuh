@@ -1,6 +1,6 @@
 // Shared device code of the Swendsen-Wang engine: lattice geometry, the per-block assign
 // phase (lcg32 draws, bonds, shared-memory union-find) and the per-block edge merge.  Used by
-// the single-lattice kernels (sw_plain.cu) and the batched persistent kernels (sw_batch.cu).
+// the single-lattice kernels (sw_plain.cu) and the batched kernels (sw_batch.cu).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -168,18 +168,6 @@ struct DrawWords {
 
 // ------------------------------------------------------------------------------------------
 // kernels
-
-// Device buffers of one lattice.
-struct LatView {
-    Geo g;
-    uint8_t *spins;
-    uint32_t *labels;
-    uint32_t *rng_state;
-    uint8_t *rng_sel;
-    uint32_t *rng_iter;
-    uint32_t *edge;
-    uint32_t thr;  // bond accept threshold, accept_threshold(p_add)
-};
 
 // Bit k of the result = bit 0 of byte k of v: multiplying the masked bytes by
 // 2^28 + 2^21 + 2^14 + 2^7 lands byte k's bit at bit 28 + k, every cross term below bit 28.
