@@ -509,7 +509,7 @@ def bench_serving(args, dist: Dist, cp) -> None:
     with ClockSampler(dist.local_rank) as clocks:
         for k, rate in enumerate((10.0, 100.0, 1000.0)):
             jobs = serving.poisson_jobs(rate, n_jobs, seed=20260 + k)
-            srv = serving.Server(32 << 30)
+            srv = serving.Server(32 << 30, device=dist.local_rank)
             try:
                 srv.run(jobs, realtime=True)
             finally:
@@ -520,7 +520,7 @@ def bench_serving(args, dist: Dist, cp) -> None:
             work += sum(j.site_updates for j in jobs if j.done is not None)
             span += s.get("makespan_s", 0.0)
         base_jobs = serving.poisson_jobs(10.0, n_jobs, seed=20260)
-        serving.SequentialServer().run(base_jobs, realtime=True)
+        serving.SequentialServer(device=dist.local_rank).run(base_jobs, realtime=True)
         base = serving.latency_summary(base_jobs)
     if dist.rank != 0:
         return
