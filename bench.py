@@ -65,27 +65,40 @@ PLAIN = {
 # distributed plumbing (control plane only: barrier and max-reduce of device times)
 
 class Dist:
+    """One process per GPU: NCCL on a GPU box (gloo where there is no GPU, as in the CPU tests).
+    Only a barrier and a max-reduce of the device-measured times go over it."""
+
     def __init__(self):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
+        self.device = None
         if self.world > 1:
             import datetime
 
+            import torch
             import torch.distributed as dist
-            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+            backend = "gloo"
+            if torch.cuda.is_available():
+                backend = "nccl"
+                torch.cuda.set_device(self.local_rank)
+                self.device = torch.device("cuda", self.local_rank)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
             self.pg = dist
 
     def barrier(self):
         if self.pg:
-            self.pg.barrier()
+            if self.device is not None:
+                self.pg.barrier(device_ids=[self.local_rank])
+            else:
+                self.pg.barrier()
 
     def max(self, x: float) -> float:
         if not self.pg:
             return x
         import torch
-        t = torch.tensor([x], dtype=torch.float64)
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
