@@ -200,7 +200,7 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
     const DrawWords<W> dw{reinterpret_cast<const uint32_t *>(smem + L.draws), L.slots};
     uint32_t *edge_s = reinterpret_cast<uint32_t *>(smem + L.edge);
     const uint8_t *sp = smem + L.sp;
-    const uint32_t BX = g.BX, BY = g.BY, NW = BX >> 5;
+    const uint32_t BX = g.BX, BY = g.BY, NW = BX >> 5, lnw = __ffs(NW) - 1;  // NW is a power of two
     uint32_t *Xw = reinterpret_cast<uint32_t *>(smem + L.bond);  // [BY][NW] x-bonds inside the block
     uint32_t *Yw = Xw + BY * NW;                                  // [BY][NW] y-bonds inside the block
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
@@ -222,7 +222,7 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
     // or on the tile's last row from the merge request's bottom edge (bits [0, TX)).  Edge bonds
     // go to edge_s (right edge: one bit per row, bottom: the row's words).
     for (uint32_t i = tid; i < BY * NW; i += blockDim.x) {
-        const uint32_t yl = i / NW, w = i - yl * NW;
+        const uint32_t yl = i >> lnw, w = i & (NW - 1);
         uint32_t X = 0, Y = 0;
         if (yl < byv) {
             const uint32_t tby = yl / TY, jj = yl - tby * TY;
@@ -266,34 +266,40 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
 
     // Scanline labelling.  Work item = (32-column strip, band of rows); a warp walks its band
     // top-down with each lane holding the provisional label of the site above.  A run (x-bonded
-    // sites of the strip row; its first lane from the gap mask below the lane, its last from the
-    // gap mask above) takes the label above its leftmost y-bonded site, or with none its own first
-    // site as a new label.  Every other y-bond of the run that meets a different label unites the
+    // sites of the strip row; its first lane from the gap mask below the lane) takes the label
+    // above its leftmost y-bonded site, or with none its own first site as a new label.  Every other y-bond of the run that meets a different label unites the
     // two in the shared union-find (toward the minimum), so each site's root is the minimum of
     // its block-local component.  Seams between strips and bands are united afterwards, then
     // every site resolves its provisional label.
     uint16_t *plab = reinterpret_cast<uint16_t *>(smem + L.plab);
-    const uint32_t nb = max(1u, nwarps / NW);                // bands
-    const uint32_t rb = (BY + nb - 1) / nb;                  // rows per band
+    const uint32_t nb = max(1u, nwarps >> lnw);              // bands
+    const uint32_t rb = (nb & (nb - 1)) == 0 ? (BY + nb - 1) >> (__ffs(nb) - 1) : (BY + nb - 1) / nb;  // rows per band
     const uint32_t below = (1u << lane) - 1u;                // lanes below this one
     for (uint32_t task = warp; task < NW * nb; task += nwarps) {
-        const uint32_t sx = task % NW, band = task / NW;
+        const uint32_t sx = task & (NW - 1), band = task >> lnw;
         const uint32_t ya = band * rb, yb = min(BY, ya + rb);
-        uint32_t above = 0xFFFFFFFFu;
-        for (uint32_t yl = ya; yl < yb; ++yl) {
-            const uint32_t X = Xw[yl * NW + sx];
-            const uint32_t Yup = yl > ya ? Yw[(yl - 1) * NW + sx] : 0u;
-            const uint32_t rs = 32 - __clz(~X & below);             // run start (lane); __clz(0) = 32
-            const uint32_t from = 0xFFFFFFFFu << rs;
-            const uint32_t re = (__ffs(~X & from) - 1) & 31u;        // run end; X bit 31 never ends a strip run
-            const uint32_t f = __ffs(Yup & from) - 1;               // leftmost y-bond from the run start, or ~0
-            const uint32_t rep = __shfl_sync(0xffffffffu, above, f & 31u);
-            const uint32_t base = yl * BX + (sx << 5);
-            const uint32_t lab = f <= re ? rep : base + rs;
-            if (((Yup >> lane) & 1u) && above != lab)
+        const uint32_t *xp = Xw + ya * NW + sx;  // this row's x-bond word; xp[BY * NW] its y-bond word
+        uint32_t base = ya * BX + (sx << 5);
+        uint32_t above = 0, Yup = 0, Xa = 0;     // the band's first row has no bonds up
+        for (uint32_t n = yb > ya ? yb - ya : 0; n != 0; --n) {
+            const uint32_t X = xp[0];
+            const uint32_t rs = 32 - __clz(~X & below);  // run start (lane); __clz(0) = 32
+            // The first y-bond or run end from the run start (bit 31 always ends a strip run):
+            // a y-bond there means the run inherits the label above it.
+            const uint32_t pos = __ffs((Yup | ~X | 0x80000000u) & (0xFFFFFFFFu << rs)) - 1;
+            const uint32_t rep = __shfl_sync(0xffffffffu, above, pos);
+            const uint32_t lab = ((Yup >> pos) & 1u) ? rep : base + rs;
+            // A y-bond whose left neighbour is bonded up too, with both rows bonded across, meets
+            // the same two runs as that neighbour's: only the leftmost of such a chain unites.
+            const uint32_t U = Yup & ~((Yup & X & Xa) << 1);
+            if (((U >> lane) & 1u) && above != lab)
                 uf_union(parent, above, lab);
             plab[base + lane] = (uint16_t)lab;
             above = lab;
+            Xa = X;
+            Yup = xp[BY * NW];
+            xp += NW;
+            base += BX;
         }
     }
     __syncthreads();
@@ -302,7 +308,7 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
     // neighbour already joins the same runs), and x-bonds from a strip's last column into the
     // next strip.
     for (uint32_t task = warp; task < (nb - 1) * NW; task += nwarps) {
-        const uint32_t sx = task % NW, yl = (task / NW + 1) * rb - 1;
+        const uint32_t sx = task & (NW - 1), yl = ((task >> lnw) + 1) * rb - 1;
         if (yl + 1 >= BY)
             continue;
         const uint32_t Y = Yw[yl * NW + sx];
@@ -314,9 +320,9 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
             uf_union(parent, plab[l], plab[l + BX]);
         }
     }
-    for (uint32_t i = tid; i < BY * (NW - 1); i += blockDim.x) {
-        const uint32_t yl = i / (NW - 1), sx = i - yl * (NW - 1);
-        if (Xw[yl * NW + sx] >> 31) {
+    for (uint32_t i = tid; i < (BY << lnw); i += blockDim.x) {
+        const uint32_t yl = i >> lnw, sx = i & (NW - 1);
+        if (sx + 1 < NW && (Xw[i] >> 31)) {
             const uint32_t l = yl * BX + (sx << 5) + 31;
             uf_union(parent, plab[l], plab[l + 1]);
         }
@@ -394,11 +400,11 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
     // ---- 1. spins of the block and its halo (column x0+bxv and row y0+byv, periodic).  Rows
     // go global -> shared by cp.async, in flight while the lcg32 draws below run; the strided
     // halo column is one byte per thread, held in a register until then.
-    const uint32_t hx = (x0 + bxv) % g.L0;
+    const uint32_t hx = x0 + bxv < g.L0 ? x0 + bxv : 0u;  // column right of the block (periodic)
     uint8_t halo = 0;
     {
         const uint32_t warp = tid >> 5, lane32 = tid & 31, nwarps = nthr >> 5;
-        const uint32_t hy = (y0 + byv) % g.L1;
+        const uint32_t hy = y0 + byv < g.L1 ? y0 + byv : 0u;  // row below the block (periodic)
         const uint32_t vec = (g.L0 % 16 == 0 && BX % 16 == 0) ? 16 : (g.L0 % 4 == 0 ? 4 : 1);
         if (vec == 16 && (BX & (BX - 1)) == 0) {
             // one 16-byte copy per thread, rows packed across the CTA (a 128-wide row is 8
@@ -446,7 +452,9 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
     // at update (2 tile_y - 1) * Ur; a tile shorter than tile_y idles through the rows it lacks.
     {
         const uint32_t tb = tid / W, lane = tid % W, lane32 = tid & 31;
-        const uint32_t tgx = bxi * g.TBX + tb % g.TBX, tgy = byi * g.TBY + tb / g.TBX;
+        // TBX is a power of two unless the caller chose the block shape
+        const uint32_t tbr = (g.TBX & (g.TBX - 1)) == 0 ? tb >> (__ffs(g.TBX) - 1) : tb / g.TBX;
+        const uint32_t tgx = bxi * g.TBX + (tb - tbr * g.TBX), tgy = byi * g.TBY + tbr;
         const bool on = tb < ntb && tgx < g.n0 && tgy < g.n1;
         const uint32_t tile = tgy * g.n0 + tgx;
         const uint32_t jjmax = on ? min(TY, g.L1 - tgy * TY) : 0;
@@ -483,11 +491,12 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
             // the rotating updates come from a mask (update k rotates iff (it + k + 1) % 15 == 0).
             // Segments of tiles off the lattice run along and store nothing.
             if (kN <= 64 && __all_sync(0xffffffffu, !on || jjmax == TYc)) {
-                uint64_t rm = 0;
-                for (uint32_t k = kShuffleDistance - 1 - it % kShuffleDistance; k < kN; k += kShuffleDistance)
-                    rm |= 1ull << k;
-                const uint64_t wm = (uint64_t)__reduce_or_sync(0xffffffffu, (uint32_t)(rm >> 32)) << 32 |
-                                    __reduce_or_sync(0xffffffffu, (uint32_t)rm);
+                // bits 14 - it % 15 + 15 j below kN (kN <= 64)
+                const uint64_t rm = (0x1000200040008001ull << (kShuffleDistance - 1 - it % kShuffleDistance)) &
+                                    (kN >= 64 ? ~0ull : (1ull << (kN & 63)) - 1);
+                uint64_t wm = __reduce_or_sync(0xffffffffu, (uint32_t)rm);
+                if constexpr (kN > 32)
+                    wm |= (uint64_t)__reduce_or_sync(0xffffffffu, (uint32_t)(rm >> 32)) << 32;
 #pragma unroll
                 for (uint32_t k = 0; k < kN; ++k) {
                     if ((wm >> k) & 1u)
@@ -495,7 +504,8 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
                     st = a * st + c;
                     const uint32_t lim = k < kRows ? TXc : TXc + TYc;          // numbers in this request
                     const uint32_t e0 = (k < kRows ? k % kUr : k - kRows) * W;  // its first element here
-                    const uint32_t word = __ballot_sync(0xffffffffu, e0 + lane < lim && lcg_accept(st, thr));
+                    const bool in = e0 + W <= lim || e0 + lane < lim;  // every lane of a full update is in
+                    const uint32_t word = __ballot_sync(0xffffffffu, in && lcg_accept(st, thr));
                     if (wr)
                         draws[k] = word;
                 }
