@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(kMergeThreads) kb_merge(BatchLat *lats, const 
         if (L->sweeps_left != 0) {
             const Geo g = L->g;
             if (threadIdx.x < g.BX + g.BY)
-                merge_block(g, (d.y >> 16) * g.nbx + (d.y & 0xFFFFu), threadIdx.x, L->edge, L->labels, fault);
+                merge_block(g, d.y & 0xFFFFu, d.y >> 16, threadIdx.x, L->edge, L->labels, fault);
         }
         d = next;
     }
@@ -734,6 +734,8 @@ int swb_batch_add(swb_batch *b, uint32_t L0, uint32_t L1, uint32_t tile_x, uint3
     if (slot == b->capacity)
         return fail(SWB_ERR_CAPACITY, "all %u lattice slots are in use", b->capacity);
     const Geo g = make_geo(L0, L1, tile_x, tile_y, b->W, kBatchThreads, block_x, block_y);
+    if (g.nbx > 0xFFFFu || g.nby > 0xFFFFu)  // block coordinates are 16-bit in the work items
+        return fail(SWB_ERR_ARGUMENT, "lattice of %u x %u sites needs more than 65535 blocks in a direction", L0, L1);
     if (assign_smem(g, b->W).total > b->smem_assign)
         return fail(SWB_ERR_ARGUMENT, "block of %u x %u sites needs more shared memory than reserved", g.BX, g.BY);
     const uint64_t bytes = lattice_bytes(g, b->W, b->series_cap);

@@ -8,6 +8,7 @@
 #include <atomic>
 #include <cstdint>
 #include <string>
+#include <utility>
 
 #include "../../include/swb200.h"
 #include "sw_device.cuh"
@@ -80,6 +81,21 @@ inline Geo make_geo(uint32_t L0, uint32_t L1, uint32_t TX, uint32_t TY, uint32_t
     return g;
 }
 
+// Updates Ks... of a sweep as straight-line code, the rotation before every update k with
+// k % 15 == kFirst (the rotating updates of a warp whose tiles share their iteration count).
+template <uint32_t kFirst, uint32_t... Ks, class Rotate, class Draw>
+__device__ __forceinline__ void draw_sequence(std::integer_sequence<uint32_t, Ks...>, Rotate &rotate, Draw &draw,
+                                              const uint32_t it)
+{
+    ((Ks % kShuffleDistance == kFirst ? rotate(it + Ks + 1, true) : (void)0, draw(Ks)), ...);
+}
+
+template <uint32_t V>
+struct U32 {  // a compile-time uint32_t passed as a value
+    static constexpr uint32_t value = V;
+};
+
+constexpr uint32_t kMaxGridY = 65535;  // block rows of a lattice: the kernels' grid y
 constexpr uint32_t kEdgeWords = 8;  // per block: [0] right edge rows, [1..4] bottom edge columns
 
 // Label encoding between the assign and flip phases of a sweep.  A block root holds its global
@@ -96,7 +112,9 @@ __device__ __forceinline__ uint32_t label_global(const Geo &g, uint32_t bxi, uin
     if (!(v & kLocalFlag))
         return v;
     const uint32_t r = v & kLocalMask;
-    return (byi * g.BY + r / g.BX) * g.L0 + bxi * g.BX + r % g.BX;
+    // BX is a power of two unless the caller chose the block shape
+    const uint32_t yl = (g.BX & (g.BX - 1)) == 0 ? r >> (__ffs(g.BX) - 1) : r / g.BX;
+    return (byi * g.BY + yl) * g.L0 + bxi * g.BX + (r - yl * g.BX);
 }
 
 struct AssignSmem {
@@ -373,7 +391,10 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
 
 // Block (bxi, byi) of a lattice: lcg32 draws, bonds, union-find in shared memory.  Runs on
 // all threads of the CTA (at least TBX * TBY * W of them); smem holds assign_smem(g, W).total bytes.
-template <int W, int TXc = 0, int TYc = 0>
+// kPhaseSeq selects the phase-dispatched draw sequence (below) for full-height tiles of a
+// compile-time shape: on B200 it is the faster form inside the batched kernel (whose item loop
+// keeps more registers live) and the slower one in the single-lattice kernel.
+template <int W, int TXc = 0, int TYc = 0, bool kPhaseSeq = false>
 __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, const uint32_t byi,
                                              const uint8_t *__restrict__ spins, uint32_t *__restrict__ labels,
                                              uint32_t *__restrict__ rng_state, uint8_t *__restrict__ rng_sel,
@@ -491,16 +512,7 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
             // the rotating updates come from a mask (update k rotates iff (it + k + 1) % 15 == 0).
             // Segments of tiles off the lattice run along and store nothing.
             if (kN <= 64 && __all_sync(0xffffffffu, !on || jjmax == TYc)) {
-                // bits 14 - it % 15 + 15 j below kN (kN <= 64)
-                const uint64_t rm = (0x1000200040008001ull << (kShuffleDistance - 1 - it % kShuffleDistance)) &
-                                    (kN >= 64 ? ~0ull : (1ull << (kN & 63)) - 1);
-                uint64_t wm = __reduce_or_sync(0xffffffffu, (uint32_t)rm);
-                if constexpr (kN > 32)
-                    wm |= (uint64_t)__reduce_or_sync(0xffffffffu, (uint32_t)(rm >> 32)) << 32;
-#pragma unroll
-                for (uint32_t k = 0; k < kN; ++k) {
-                    if ((wm >> k) & 1u)
-                        rotate(it + k + 1, (rm >> k) & 1u);
+                auto draw = [&](const uint32_t k) {  // update k of the sweep and its ballot
                     st = a * st + c;
                     const uint32_t lim = k < kRows ? TXc : TXc + TYc;          // numbers in this request
                     const uint32_t e0 = (k < kRows ? k % kUr : k - kRows) * W;  // its first element here
@@ -508,6 +520,51 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
                     const uint32_t word = __ballot_sync(0xffffffffu, in && lcg_accept(st, thr));
                     if (wr)
                         draws[k] = word;
+                };
+                // The tiles of a warp normally share their iteration count (every full-height tile
+                // makes kN updates a sweep): then the rotating updates sit at compile-time
+                // positions, one straight-line sequence per phase it % 15 (kPhaseSeq; tiles off the
+                // lattice take the phase of the first tile on it, their results are not stored).
+                // Otherwise update k rotates a tile iff bit k of its mask is set.
+                bool seq = false;
+                if constexpr (kPhaseSeq) {
+                    const uint32_t itu = __shfl_sync(0xffffffffu, it, (__ffs(__ballot_sync(0xffffffffu, on)) - 1) & 31);
+                    if (__all_sync(0xffffffffu, !on || it == itu)) {
+                        auto run = [&](auto phase) {
+                            draw_sequence<decltype(phase)::value>(std::make_integer_sequence<uint32_t, kN>{}, rotate, draw, itu);
+                        };
+                        switch (kShuffleDistance - 1 - itu % kShuffleDistance) {
+                        case 0: run(U32<0>{}); break;
+                        case 1: run(U32<1>{}); break;
+                        case 2: run(U32<2>{}); break;
+                        case 3: run(U32<3>{}); break;
+                        case 4: run(U32<4>{}); break;
+                        case 5: run(U32<5>{}); break;
+                        case 6: run(U32<6>{}); break;
+                        case 7: run(U32<7>{}); break;
+                        case 8: run(U32<8>{}); break;
+                        case 9: run(U32<9>{}); break;
+                        case 10: run(U32<10>{}); break;
+                        case 11: run(U32<11>{}); break;
+                        case 12: run(U32<12>{}); break;
+                        case 13: run(U32<13>{}); break;
+                        default: run(U32<14>{}); break;
+                        }
+                        seq = true;
+                    }
+                }
+                if (!seq) {
+                    const uint64_t rm = (0x1000200040008001ull << (kShuffleDistance - 1 - it % kShuffleDistance)) &
+                                        (kN >= 64 ? ~0ull : (1ull << (kN & 63)) - 1);
+                    uint64_t wm = __reduce_or_sync(0xffffffffu, (uint32_t)rm);
+                    if constexpr (kN > 32)
+                        wm |= (uint64_t)__reduce_or_sync(0xffffffffu, (uint32_t)(rm >> 32)) << 32;
+#pragma unroll
+                    for (uint32_t k = 0; k < kN; ++k) {
+                        if ((wm >> k) & 1u)
+                            rotate(it + k + 1, (rm >> k) & 1u);
+                        draw(k);
+                    }
                 }
                 it += kN;
                 fast = true;
@@ -658,11 +715,11 @@ __device__ __forceinline__ void assign_block_any(const Geo &g, const uint32_t bx
 {
 #define SWB_TILE(tx, ty)                                                                                              \
     if (g.TX == tx && g.TY == ty) {                                                                                   \
-        assign_block<W, tx, ty>(g, bxi, byi, spins, labels, rng_state, rng_sel, rng_iter, thr, edge, nullptr, nullptr, \
-                                smem);                                                                                \
+        assign_block<W, tx, ty, true>(g, bxi, byi, spins, labels, rng_state, rng_sel, rng_iter, thr, edge, nullptr, \
+                                      nullptr, smem);                                                                 \
         return;                                                                                                       \
     }
-    if (W == 16) {
+    if constexpr (W == 16) {
         SWB_TILE(16, 8)
         SWB_TILE(8, 8)
         SWB_TILE(32, 4)
@@ -675,22 +732,21 @@ __device__ __forceinline__ void assign_block_any(const Geo &g, const uint32_t bx
     assign_block<W>(g, bxi, byi, spins, labels, rng_state, rng_sel, rng_iter, thr, edge, nullptr, nullptr, smem);
 }
 
-// Unions across the right and bottom edge (periodic) of block blk: thread t < BY takes row
-// t of the right edge, BY <= t < BY + BX column t - BY of the bottom edge.
-__device__ __forceinline__ void merge_block(const Geo &g, const uint32_t blk, const uint32_t t,
+// Unions across the right and bottom edge (periodic) of block (bxi, byi): thread t < BY takes
+// row t of the right edge, BY <= t < BY + BX column t - BY of the bottom edge.
+__device__ __forceinline__ void merge_block(const Geo &g, const uint32_t bxi, const uint32_t byi, const uint32_t t,
                                             const uint32_t *__restrict__ edge, uint32_t *labels, unsigned int *fault)
 {
-    const uint32_t bxi = blk % g.nbx, byi = blk / g.nbx;
     const uint32_t x0 = bxi * g.BX, y0 = byi * g.BY;
     const uint32_t bxv = min(g.BX, g.L0 - x0), byv = min(g.BY, g.L1 - y0);
-    const uint32_t *e = edge + (size_t)blk * kEdgeWords;
+    const uint32_t *e = edge + ((size_t)byi * g.nbx + bxi) * kEdgeWords;
     size_t s = 0, nb = 0;
     uint32_t nbx = bxi, nby = byi;  // block of the neighbour site
     bool go = false;
     if (t < g.BY) {
         if (t < byv && ((e[0] >> t) & 1u)) {
             s = (size_t)(y0 + t) * g.L0 + x0 + bxv - 1;
-            nb = (size_t)(y0 + t) * g.L0 + (x0 + bxv) % g.L0;
+            nb = (size_t)(y0 + t) * g.L0 + (x0 + bxv < g.L0 ? x0 + bxv : 0u);
             nbx = bxi + 1 == g.nbx ? 0 : bxi + 1;
             go = true;
         }
@@ -698,7 +754,7 @@ __device__ __forceinline__ void merge_block(const Geo &g, const uint32_t blk, co
         const uint32_t xl = t - g.BY;
         if (xl < bxv && ((e[1 + (xl >> 5)] >> (xl & 31)) & 1u)) {
             s = (size_t)(y0 + byv - 1) * g.L0 + x0 + xl;
-            nb = (size_t)((y0 + byv) % g.L1) * g.L0 + x0 + xl;
+            nb = (size_t)(y0 + byv < g.L1 ? y0 + byv : 0u) * g.L0 + x0 + xl;
             nby = byi + 1 == g.nby ? 0 : byi + 1;
             go = true;
         }
@@ -733,11 +789,14 @@ __device__ __forceinline__ void flip_block(const Geo &g, const uint32_t bxi, con
     const uint32_t bxv = min(BX, L0 - x0), byv = min(g.BY, g.L1 - y0);
     const uint32_t base = y0 * L0 + x0;
     const uint32_t nq = (bxv >> 2) * byv, qrow = bxv >> 2;
-    if ((L0 & 3u) == 0 && qrow && blockDim.x % qrow == 0 && nq <= kQuads * blockDim.x) {
+    // quads per row: a power of two (32 in a full 128-wide block) takes the shift path below
+    const bool qpow2 = qrow && (qrow & (qrow - 1)) == 0;
+    if ((L0 & 3u) == 0 && qpow2 && (blockDim.x & (qrow - 1)) == 0 && nq <= kQuads * blockDim.x) {
         // Every thread holds at most kQuads quads (4 labels + 4 spins each) in registers: one
         // round trip for the loads, the merged roots' chains, then the flips.  Quad k of a
-        // thread is column xq of row yl0 + k * rstep (whole rows per step, so no division).
-        const uint32_t rstep = blockDim.x / qrow, yl0 = tid / qrow, xq4 = 4 * (tid - yl0 * qrow);
+        // thread is column xq of row yl0 + k * rstep (whole rows per step).
+        const uint32_t lq = __ffs(qrow) - 1;
+        const uint32_t rstep = blockDim.x >> lq, yl0 = tid >> lq, xq4 = 4 * (tid & (qrow - 1));
         uint4 lab[kQuads];
         uint32_t spn[kQuads];
 #pragma unroll

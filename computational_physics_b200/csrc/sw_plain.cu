@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(kAssignThreads, 4) k_assign(const Geo g, const
 __global__ void __launch_bounds__(256) k_merge(const Geo g, const uint32_t *__restrict__ edge, uint32_t *labels,
                                                unsigned int *fault)
 {
-    merge_block(g, blockIdx.x, threadIdx.x, edge, labels, fault);
+    merge_block(g, blockIdx.x, blockIdx.y, threadIdx.x, edge, labels, fault);
 }
 
 // Resolve + flip, one CTA per block (flip_block).
@@ -270,7 +270,7 @@ int launch_assign_w(swb_lattice *h, float p_add, uint8_t *dbg_bonds, uint32_t *d
 {
     if (dbg_assign)
         return launch_assign_k<W, 0, 0, true>(h, p_add, dbg_bonds, dbg_assign);
-    if (W == 16) {
+    if constexpr (W == 16) {
         const uint32_t tx = h->g.TX, ty = h->g.TY;
         if (tx == 16 && ty == 8) return launch_assign_k<W, 16, 8, false>(h, p_add, nullptr, nullptr);
         if (tx == 8 && ty == 8) return launch_assign_k<W, 8, 8, false>(h, p_add, nullptr, nullptr);
@@ -298,7 +298,7 @@ int launch_sweep(swb_lattice *h, float p_add, bool write_labels, uint8_t *dbg_bo
     int rc = launch_assign(h, p_add, dbg_bonds, dbg_assign);
     if (rc)
         return rc;
-    k_merge<<<h->n_blocks, h->g.BX + h->g.BY, 0, h->stream>>>(h->g, h->edge, h->labels, h->fault);
+    k_merge<<<dim3(h->g.nbx, h->g.nby), h->g.BX + h->g.BY, 0, h->stream>>>(h->g, h->edge, h->labels, h->fault);
     SWB_LAUNCHED();
     if (write_labels)
         k_flip<true><<<dim3(h->g.nbx, h->g.nby), kFlipThreads, h->smem_flip, h->stream>>>(h->g, h->spins, h->labels, h->fault);
@@ -379,6 +379,8 @@ int swb_create(swb_lattice **out, uint32_t L0, uint32_t L1, uint32_t tile_x, uin
         return fail(SWB_ERR_ARGUMENT, "unsupported tile %u x %u (tile_x in {8,16,32}, 2 <= tile_y <= 32)", tile_x, tile_y);
     if (!valid_width(lcg_width))
         return fail(SWB_ERR_ARGUMENT, "unsupported lcg32 width %u (8, 16 or 32)", lcg_width);
+    if (make_geo(L0, L1, tile_x, tile_y, lcg_width, kAssignThreads).nby > kMaxGridY)
+        return fail(SWB_ERR_ARGUMENT, "lattice of %u rows needs more than %u block rows", L1, kMaxGridY);
     swb_lattice *h = new swb_lattice();
     h->device = device;
     h->W = lcg_width;
@@ -720,7 +722,7 @@ int swb_sweep_timed(swb_lattice *h, float temperature, uint32_t n_sweeps, int pe
         if ((rc = launch_assign(h, p_add, nullptr, nullptr)))
             break;
         SWB_CUDA(cudaEventRecord(ev[2], h->stream));
-        k_merge<<<h->n_blocks, h->g.BX + h->g.BY, 0, h->stream>>>(h->g, h->edge, h->labels, h->fault);
+        k_merge<<<dim3(h->g.nbx, h->g.nby), h->g.BX + h->g.BY, 0, h->stream>>>(h->g, h->edge, h->labels, h->fault);
         SWB_LAUNCHED();
         SWB_CUDA(cudaEventRecord(ev[3], h->stream));
         k_flip<false><<<dim3(h->g.nbx, h->g.nby), kFlipThreads, h->smem_flip, h->stream>>>(h->g, h->spins, h->labels, h->fault);
@@ -858,6 +860,8 @@ int swb_sweep_static(void *stream, uint32_t L0, uint32_t L1, uint32_t tile_x, ui
         return fail(SWB_ERR_ARGUMENT, "unsupported lcg32 width %u (8, 16 or 32)", lcg_width);
     if (!(temperature > 0.0f) || !std::isfinite(temperature))
         return fail(SWB_ERR_ARGUMENT, "temperature must be positive and finite");
+    if (make_geo(L0, L1, tile_x, tile_y, lcg_width, kAssignThreads).nby > kMaxGridY)
+        return fail(SWB_ERR_ARGUMENT, "lattice of %u rows needs more than %u block rows", L1, kMaxGridY);
 
     swb_lattice h;  // a view: caller's buffers plus the static scratch; owns nothing
     h.stream = static_cast<cudaStream_t>(stream);

@@ -55,6 +55,8 @@ def test_pure_host_entry_points_without_gpu():
     assert "evenly sized" in lib.swb_last_error().decode()
     assert lib.swb_create(ctypes.byref(h), 16, 16, 12, 8, 16, 1, 0) == 1          # tile width
     assert lib.swb_create(ctypes.byref(h), 16, 16, 16, 8, 12, 1, 0) == 1          # lcg width
+    assert lib.swb_create(ctypes.byref(h), 2, 4_200_000, 8, 32, 16, 1, 0) == 1     # > 65535 block rows
+    assert "block rows" in lib.swb_last_error().decode()
     assert not h.value
 
 
