@@ -187,12 +187,12 @@ def assign_bytes(n_sites: int, n_tiles: int, W: int) -> float:
 
 # DRAM traffic of one assign pass over a workload (dram__bytes_read.sum + dram__bytes_write.sum)
 # from one ncu capture of the same kernel, per site: the batched mix of 512 lattices (39,603,200
-# sites; the round runs its two lattice groups as two launches: 33,179,392 + 33,145,344 B read,
-# 60,603,136 + 64,940,032 B written) and one 8192 x 8192 lattice, tile 16 x 8 (111,338,496 B read
-# + 253,723,904 B written).  Traffic grows with the sites swept, so other sizes scale by their
+# sites; the round runs its two lattice groups as two launches: 33,100,288 + 33,114,624 B read,
+# 38,437,632 + 40,070,912 B written) and one 8192 x 8192 lattice, tile 16 x 8 (111,201,792 B read
+# + 254,913,792 B written).  Traffic grows with the sites swept, so other sizes scale by their
 # site count.
-ASSIGN_TRAFFIC_PER_SITE = {"kb_assign": (33_179_392 + 33_145_344 + 60_603_136 + 64_940_032) / 39_603_200,
-                           "k_assign": (111_338_496 + 253_723_904) / 8192 ** 2}
+ASSIGN_TRAFFIC_PER_SITE = {"kb_assign": (33_100_288 + 33_114_624 + 38_437_632 + 40_070_912) / 39_603_200,
+                           "k_assign": (111_201_792 + 254_913_792) / 8192 ** 2}
 
 
 def flip_bytes(n_sites: int) -> float:
