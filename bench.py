@@ -378,7 +378,7 @@ def bench_plain(args, dist: Dist, cp) -> dict:
                      "unit": "GB/s", "frac": ab / (a_ms / 1e3) / 1e9 / peak,
                      "traffic": ASSIGN_TRAFFIC_PER_SITE["k_assign"] * n, "peak_kind": peak_kind,
                      "bytes_per_launch": ab, "ms_per_launch": a_ms},
-        "kernels_ms_per_sweep": {"assign": a_ms, "merge": float(k[2]) / nk, "flip": float(k[3]) / nk},
+        "kernels_ms_per_sweep": {"assign": a_ms, "merge": float(k[2]) / nk, "resolve_flip": float(k[3]) / nk},
         "flip_GBs": fb / (float(k[3]) / nk / 1e3) / 1e9,
         "e2e": {"value": e2e, "unit": "spin-updates/s", "h2d_bytes_per_step": n, "d2h_bytes_per_step": n + 16},
     }
@@ -495,7 +495,7 @@ def bench_batched(args, dist: Dist, cp) -> dict:
                      "unit": "GB/s", "frac": ab / (a_ms / 1e3) / 1e9 / peak,
                      "traffic": ASSIGN_TRAFFIC_PER_SITE["kb_assign"] * sites, "peak_kind": peak_kind,
                      "bytes_per_launch": ab, "ms_per_launch": a_ms},
-        "kernels_ms_per_sweep": {"assign": a_ms, "merge": float(k[2]) / nk, "flip": float(k[3]) / nk},
+        "kernels_ms_per_sweep": {"assign": a_ms, "merge": float(k[2]) / nk, "resolve_flip": float(k[3]) / nk},
         "e2e": {"value": dist.world * sites * e2e_steps / e2e_s, "unit": "spin-updates/s",
                 "h2d_bytes_per_step": sites, "d2h_bytes_per_step": sites},
         "tiles": {str(L): [list(t), list(bl)] for (L, _, _), (t, bl) in sorted(zip(mix, tiles))},

@@ -2,8 +2,8 @@
 // tiles and temperatures advance together, one kernel launch per sweep phase for all of them.
 //
 // Work items.  Every active lattice contributes its blocks (TBX x TBY tiles) to one flat list
-// of block items (lattice slot, block coordinates), big lattices first.  kb_assign / kb_merge
-// / kb_flip run one CTA per item (a CTA takes items blockIdx.x, blockIdx.x + gridDim.x, ...,
+// of block items (lattice slot, block coordinates), big lattices first.  kb_assign, kb_merge,
+// kb_resolve and kb_flip run one CTA per item (a CTA takes items blockIdx.x, blockIdx.x + gridDim.x, ...,
 // loading the next item's descriptor while it works on the current one, so a smaller grid
 // also covers the list); kb_measure pulls chunks of 4096 sites from a device counter
 // (atomicAdd), which kb_assign resets.  A sweep needs no host work and is one CUDA graph: the
@@ -42,6 +42,7 @@ struct BatchLat {
     uint8_t *rng_sel;
     uint32_t *rng_iter;
     uint32_t *edge;
+    uint32_t *linked;         // merge slots: the root each edge union linked
     Obs *obs;
     long long *series;
     unsigned long long series_cap;
@@ -121,14 +122,31 @@ __global__ void __launch_bounds__(kMergeThreads) kb_merge(BatchLat *lats, const 
         if (L->sweeps_left != 0) {
             const Geo g = L->g;
             if (threadIdx.x < g.BX + g.BY)
-                merge_block(g, d.y & 0xFFFFu, d.y >> 16, threadIdx.x, L->edge, L->labels, fault);
+                merge_block(g, d.y & 0xFFFFu, d.y >> 16, threadIdx.x, L->edge, L->labels, fault, L->linked);
         }
         d = next;
     }
 }
 
-// Resolve + flip of one block (flip_block); the last block of a lattice closes its round
-// (sweep count and budget).
+// ResolveLabels for the roots each block's merge linked (resolve_block).
+__global__ void __launch_bounds__(kMergeThreads) kb_resolve(BatchLat *lats, const uint2 *items, const uint32_t total,
+                                                            unsigned int *fault)
+{
+    uint2 d = load_item(items, blockIdx.x, total);
+    for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
+        const uint2 next = load_item(items, item + gridDim.x, total);
+        const BatchLat *L = lats + d.x;
+        if (L->sweeps_left != 0) {
+            const Geo g = L->g;
+            if (threadIdx.x < g.BX + g.BY)
+                resolve_block(g, d.y & 0xFFFFu, d.y >> 16, threadIdx.x, L->linked, L->labels, fault);
+        }
+        d = next;
+    }
+}
+
+// Flip of one block (flip_block, after kb_resolve); the last block of a lattice closes its
+// round (sweep count and budget).
 __global__ void __launch_bounds__(kFlipThreads, 6) kb_flip(BatchLat *lats, const uint2 *items, const uint32_t total,
                                                             unsigned int *fault)
 {
@@ -139,7 +157,7 @@ __global__ void __launch_bounds__(kFlipThreads, 6) kb_flip(BatchLat *lats, const
         BatchLat *L = lats + d.x;
         if (L->sweeps_left != 0) {
             const Geo g = L->g;
-            flip_block<false, 4>(g, d.y & 0xFFFFu, d.y >> 16, L->spins, L->labels, fault, smem);
+            flip_block<false, 4, true>(g, d.y & 0xFFFFu, d.y >> 16, L->spins, L->labels, fault, smem);
             __syncthreads();
             if (threadIdx.x == 0) {
                 __threadfence();
@@ -392,7 +410,7 @@ uint64_t lattice_bytes(const Geo &g, uint32_t W, uint64_t series_cap)
     const uint64_t n = (uint64_t)g.L0 * g.L1, tiles = (uint64_t)g.n0 * g.n1, blocks = (uint64_t)g.nbx * g.nby;
     auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
     return al(n) + al(4 * n) + al(4 * tiles * W) + al(tiles * W) + al(4 * tiles) + al(4 * kEdgeWords * blocks) +
-           al(sizeof(Obs)) + al(16 * series_cap);
+           al(4 * (uint64_t)(g.BX + g.BY) * blocks) + al(sizeof(Obs)) + al(16 * series_cap);
 }
 
 int upload_descriptor(swb_batch *b, uint32_t id)
@@ -501,6 +519,13 @@ int launch_merge_b(swb_batch *b, const uint2 *items, uint32_t n, cudaStream_t st
     return SWB_OK;
 }
 
+int launch_resolve_b(swb_batch *b, const uint2 *items, uint32_t n, cudaStream_t st)
+{
+    kb_resolve<<<std::max(n, 1u), kMergeThreads, 0, st>>>(b->d_lats, items, n, b->d_fault);
+    SWB_LAUNCHED();
+    return SWB_OK;
+}
+
 int launch_flip_b(swb_batch *b, const uint2 *items, uint32_t n, cudaStream_t st)
 {
     kb_flip<<<std::max(n, 1u), kFlipThreads, b->smem_flip, st>>>(b->d_lats, items, n, b->d_fault);
@@ -508,12 +533,14 @@ int launch_flip_b(swb_batch *b, const uint2 *items, uint32_t n, cudaStream_t st)
     return SWB_OK;
 }
 
-// The three phases of one sweep over a list of block items.
+// The phases of one sweep over a list of block items.
 int launch_phases_b(swb_batch *b, const uint2 *items, uint32_t n, cudaStream_t st)
 {
     if (int rc = launch_assign_b(b, items, n, st))
         return rc;
     if (int rc = launch_merge_b(b, items, n, st))
+        return rc;
+    if (int rc = launch_resolve_b(b, items, n, st))
         return rc;
     return launch_flip_b(b, items, n, st);
 }
@@ -756,6 +783,7 @@ int swb_batch_add(swb_batch *b, uint32_t L0, uint32_t L1, uint32_t tile_x, uint3
     d.rng_sel = reinterpret_cast<uint8_t *>(p); p += al(tiles * b->W);
     d.rng_iter = reinterpret_cast<uint32_t *>(p); p += al(4 * tiles);
     d.edge = reinterpret_cast<uint32_t *>(p); p += al(4 * kEdgeWords * blocks);
+    d.linked = reinterpret_cast<uint32_t *>(p); p += al(4 * (uint64_t)(g.BX + g.BY) * blocks);
     d.obs = reinterpret_cast<Obs *>(p); p += al(sizeof(Obs));
     d.series = reinterpret_cast<long long *>(p);
     d.series_cap = b->series_cap;
@@ -949,6 +977,9 @@ int swb_batch_sweep_timed(swb_batch *b, uint32_t n_rounds, int per_kernel, float
             if ((rc = launch_merge_b(b, b->d_items, b->items_n, b->stream)))
                 break;
             SWB_CUDA(cudaEventRecord(ev[3], b->stream));
+            // resolve + flip: the reference's ResolveLabels and FlipClusters
+            if ((rc = launch_resolve_b(b, b->d_items, b->items_n, b->stream)))
+                break;
             if ((rc = launch_flip_b(b, b->d_items, b->items_n, b->stream)))
                 break;
             SWB_CUDA(cudaEventRecord(ev[4], b->stream));

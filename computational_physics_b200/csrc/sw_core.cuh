@@ -733,9 +733,12 @@ __device__ __forceinline__ void assign_block_any(const Geo &g, const uint32_t bx
 }
 
 // Unions across the right and bottom edge (periodic) of block (bxi, byi): thread t < BY takes
-// row t of the right edge, BY <= t < BY + BX column t - BY of the bottom edge.
+// row t of the right edge, BY <= t < BY + BX column t - BY of the bottom edge.  With `linked`,
+// slot t of the block's BX + BY slots receives the root this thread's union linked (kNoLink
+// for none): every block root the merge turns into a non-root appears in exactly one slot.
 __device__ __forceinline__ void merge_block(const Geo &g, const uint32_t bxi, const uint32_t byi, const uint32_t t,
-                                            const uint32_t *__restrict__ edge, uint32_t *labels, unsigned int *fault)
+                                            const uint32_t *__restrict__ edge, uint32_t *labels, unsigned int *fault,
+                                            uint32_t *__restrict__ linked)
 {
     const uint32_t x0 = bxi * g.BX, y0 = byi * g.BY;
     const uint32_t bxv = min(g.BX, g.L0 - x0), byv = min(g.BY, g.L1 - y0);
@@ -759,12 +762,29 @@ __device__ __forceinline__ void merge_block(const Geo &g, const uint32_t bxi, co
             go = true;
         }
     }
+    uint32_t link = kNoLink;
     if (go) {
         const volatile uint32_t *vl = labels;
         const uint32_t a = label_global(g, bxi, byi, vl[s]), b = label_global(g, nbx, nby, vl[nb]);
         if (a != b)
-            guf_union_pair(labels, a, b, fault);
+            link = guf_union_pair(labels, a, b, fault);
     }
+    if (linked)
+        linked[((size_t)byi * g.nbx + bxi) * (g.BX + g.BY) + t] = link;
+}
+
+// ResolveLabels for the roots the merge linked (slot t of block (bxi, byi), after every merge
+// of the sweep): the root's chain is walked to the cluster's root, which is stored in its
+// label.  Afterwards every block root's label is its cluster's root, so the flip needs no
+// chase; the chases of all blocks are in flight together here instead of behind each flip
+// CTA's barrier.
+__device__ __forceinline__ void resolve_block(const Geo &g, const uint32_t bxi, const uint32_t byi, const uint32_t t,
+                                              const uint32_t *__restrict__ linked, uint32_t *labels,
+                                              unsigned int *fault)
+{
+    const uint32_t b = linked[((size_t)byi * g.nbx + bxi) * (g.BX + g.BY) + t];
+    if (b != kNoLink)
+        labels[b] = guf_find(labels, b, fault);  // the tree's minimum: other finds' atomicMin never undo it
 }
 
 // Shared memory of flip_block: the resolved label of every block root.
@@ -775,10 +795,10 @@ __host__ __device__ inline uint32_t flip_smem_bytes(const Geo &g)
 
 // ResolveLabels + FlipClusters for block (bxi, byi) after the merge.  Block roots (labels
 // without kLocalFlag) follow their chain once (guf_find, which also compresses it for the other
-// blocks) into shared memory; every site then reads its root's result there and flips iff the
-// cluster's label is odd.  kWriteLabels stores the resolved global labels (the reference's
-// ResolveLabels output).
-template <bool kWriteLabels, int kQuads = 2>
+// blocks) into shared memory, or with kResolved (resolve_block ran) take their label as it is;
+// every site then reads its root's result there and flips iff the cluster's label is odd.
+// kWriteLabels stores the resolved global labels (the reference's ResolveLabels output).
+template <bool kWriteLabels, int kQuads = 2, bool kResolved = false>
 __device__ __forceinline__ void flip_block(const Geo &g, const uint32_t bxi, const uint32_t byi, uint8_t *spins,
                                            uint32_t *labels, unsigned int *fault, unsigned char *smem)
 {
@@ -817,7 +837,7 @@ __device__ __forceinline__ void flip_block(const Geo &g, const uint32_t bxi, con
 #pragma unroll
                 for (int j = 0; j < 4; ++j)
                     if (!(v[j] & kLocalFlag))  // a block root: v is its parent (itself unless merged)
-                        res[l + j] = v[j] == s + j ? v[j] : guf_find(labels, v[j], fault);
+                        res[l + j] = kResolved || v[j] == s + j ? v[j] : guf_find(labels, v[j], fault);
             }
         }
         __syncthreads();
@@ -845,7 +865,7 @@ __device__ __forceinline__ void flip_block(const Geo &g, const uint32_t bxi, con
             const uint32_t site = base + yl * L0 + xl;
             const uint32_t v = labels[site];
             if (!(v & kLocalFlag))
-                res[yl * BX + xl] = v == site ? v : guf_find(labels, v, fault);
+                res[yl * BX + xl] = kResolved || v == site ? v : guf_find(labels, v, fault);
         }
     __syncthreads();
     if ((L0 & 3u) == 0) {

@@ -191,10 +191,14 @@ __device__ __forceinline__ void guf_union(uint32_t *p, uint32_t a, uint32_t b, u
     atomicOr(fault, 2u);
 }
 
+constexpr uint32_t kNoLink = 0xFFFFFFFFu;  // guf_union_pair linked no root
+
 // The same union with the two root walks advancing together, one level per step, so the loads
 // of both chains are in flight at once.  Each step also points the node it leaves at its
-// grandparent (path splitting, by atomicMin as above).  Same caps and fault bits.
-__device__ __forceinline__ void guf_union_pair(uint32_t *p, uint32_t a, uint32_t b, unsigned int *fault)
+// grandparent (path splitting, by atomicMin as above).  Same caps and fault bits.  Returns the
+// root it linked below the other (each root is linked at most once: afterwards it is no root),
+// or kNoLink when the two were already one tree.
+__device__ __forceinline__ uint32_t guf_union_pair(uint32_t *p, uint32_t a, uint32_t b, unsigned int *fault)
 {
     const volatile uint32_t *vp = p;
     for (uint32_t n = 0; n < kUnionRetryCap; ++n) {
@@ -202,7 +206,7 @@ __device__ __forceinline__ void guf_union_pair(uint32_t *p, uint32_t a, uint32_t
         for (uint32_t k = 0; ya != a || yb != b; ++k) {
             if (k >= kChainCap) {
                 atomicOr(fault, 1u);
-                return;
+                return kNoLink;
             }
             const uint32_t za = ya != a ? vp[ya] : ya;
             const uint32_t zb = yb != b ? vp[yb] : yb;
@@ -220,7 +224,7 @@ __device__ __forceinline__ void guf_union_pair(uint32_t *p, uint32_t a, uint32_t
             }
         }
         if (a == b)
-            return;
+            return kNoLink;
         if (a > b) {
             const uint32_t t = a;
             a = b;
@@ -228,10 +232,11 @@ __device__ __forceinline__ void guf_union_pair(uint32_t *p, uint32_t a, uint32_t
         }
         const uint32_t old = atomicMin(p + b, a);
         if (old == b)
-            return;
+            return b;
         b = old;
     }
     atomicOr(fault, 2u);
+    return kNoLink;
 }
 
 }  // namespace swb

@@ -15,9 +15,12 @@
 //             A recorded sweep (kDebug) labels tile by tile first, as the reference's
 //             AssignLabels does, to dump that stage.
 //   k_merge   [MergeLabels across blocks]  atomicMin union on the global label array for
-//             the edge bonds recorded by k_assign.
-//   k_flip    [ResolveLabels + FlipClusters]  each merged block root's chain is walked once
-//             to the root (the cluster's minimum site index); spin ^= root & 1.
+//             the edge bonds recorded by k_assign; each union records the root it linked.
+//   k_resolve [ResolveLabels]  every linked root's chain is walked once to the root (the
+//             cluster's minimum site index), which becomes its label.
+//   k_flip    [ResolveLabels + FlipClusters]  every site reads its block root's label;
+//             spin ^= root & 1.  (The static-scratch entry point has no room for the linked
+//             roots: its k_flip walks the merged roots' chains itself, without k_resolve.)
 //
 // k_measure (every measure_every-th sweep) reduces energy and magnetisation on the device
 // and accumulates E, E^2, |M| in FP64 (Lattice<2>::GetEnergyAndMagnetization,
@@ -78,20 +81,27 @@ __global__ void __launch_bounds__(kAssignThreads, 4) k_assign(const Geo g, const
 }
 
 __global__ void __launch_bounds__(256) k_merge(const Geo g, const uint32_t *__restrict__ edge, uint32_t *labels,
-                                               unsigned int *fault)
+                                               unsigned int *fault, uint32_t *__restrict__ linked)
 {
-    merge_block(g, blockIdx.x, blockIdx.y, threadIdx.x, edge, labels, fault);
+    merge_block(g, blockIdx.x, blockIdx.y, threadIdx.x, edge, labels, fault, linked);
+}
+
+// The linked roots of one block's merge slots (resolve_block), one thread per slot.
+__global__ void __launch_bounds__(256) k_resolve(const Geo g, const uint32_t *__restrict__ linked, uint32_t *labels,
+                                                 unsigned int *fault)
+{
+    resolve_block(g, blockIdx.x, blockIdx.y, threadIdx.x, linked, labels, fault);
 }
 
 // Resolve + flip, one CTA per block (flip_block).
 constexpr uint32_t kFlipThreads = 256;  // 6 CTAs per SM (40 registers), four quads of a 128 x 32 block per thread
 
-template <bool kWriteLabels>
+template <bool kWriteLabels, bool kResolved>
 __global__ void __launch_bounds__(kFlipThreads, 6) k_flip(const Geo g, uint8_t *__restrict__ spins, uint32_t *labels,
                                                        unsigned int *fault)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    flip_block<kWriteLabels, 4>(g, blockIdx.x, blockIdx.y, spins, labels, fault, smem);
+    flip_block<kWriteLabels, 4, kResolved>(g, blockIdx.x, blockIdx.y, spins, labels, fault, smem);
 }
 
 __global__ void __launch_bounds__(256) k_measure(const uint32_t L0, const uint32_t L1, const uint8_t *__restrict__ spins,
@@ -234,6 +244,7 @@ struct swb_lattice {
     uint8_t *rng_sel = nullptr;
     uint32_t *rng_iter = nullptr;
     uint32_t *edge = nullptr;
+    uint32_t *linked = nullptr;  // merge slots: the root each edge union linked (null: flip chases)
     Obs *obs = nullptr;
     long long *series = nullptr;
     unsigned long long series_cap = 0;
@@ -293,19 +304,43 @@ int launch_assign(swb_lattice *h, float p_add, uint8_t *dbg_bonds, uint32_t *dbg
     return fail(SWB_ERR_ARGUMENT, "unsupported lcg width %u", h->W);
 }
 
-int launch_sweep(swb_lattice *h, float p_add, bool write_labels, uint8_t *dbg_bonds, uint32_t *dbg_assign)
+int launch_merge(swb_lattice *h)
 {
-    int rc = launch_assign(h, p_add, dbg_bonds, dbg_assign);
-    if (rc)
-        return rc;
-    k_merge<<<dim3(h->g.nbx, h->g.nby), h->g.BX + h->g.BY, 0, h->stream>>>(h->g, h->edge, h->labels, h->fault);
+    const dim3 grid(h->g.nbx, h->g.nby);
+    k_merge<<<grid, h->g.BX + h->g.BY, 0, h->stream>>>(h->g, h->edge, h->labels, h->fault, h->linked);
     SWB_LAUNCHED();
-    if (write_labels)
-        k_flip<true><<<dim3(h->g.nbx, h->g.nby), kFlipThreads, h->smem_flip, h->stream>>>(h->g, h->spins, h->labels, h->fault);
-    else
-        k_flip<false><<<dim3(h->g.nbx, h->g.nby), kFlipThreads, h->smem_flip, h->stream>>>(h->g, h->spins, h->labels, h->fault);
+    if (h->linked) {
+        k_resolve<<<grid, h->g.BX + h->g.BY, 0, h->stream>>>(h->g, h->linked, h->labels, h->fault);
+        SWB_LAUNCHED();
+    }
+    return SWB_OK;
+}
+
+int launch_flip(swb_lattice *h, bool write_labels)
+{
+    const dim3 grid(h->g.nbx, h->g.nby);
+    if (h->linked) {
+        if (write_labels)
+            k_flip<true, true><<<grid, kFlipThreads, h->smem_flip, h->stream>>>(h->g, h->spins, h->labels, h->fault);
+        else
+            k_flip<false, true><<<grid, kFlipThreads, h->smem_flip, h->stream>>>(h->g, h->spins, h->labels, h->fault);
+    } else {
+        if (write_labels)
+            k_flip<true, false><<<grid, kFlipThreads, h->smem_flip, h->stream>>>(h->g, h->spins, h->labels, h->fault);
+        else
+            k_flip<false, false><<<grid, kFlipThreads, h->smem_flip, h->stream>>>(h->g, h->spins, h->labels, h->fault);
+    }
     SWB_LAUNCHED();
     return SWB_OK;
+}
+
+int launch_sweep(swb_lattice *h, float p_add, bool write_labels, uint8_t *dbg_bonds, uint32_t *dbg_assign)
+{
+    if (int rc = launch_assign(h, p_add, dbg_bonds, dbg_assign))
+        return rc;
+    if (int rc = launch_merge(h))
+        return rc;
+    return launch_flip(h, write_labels);
 }
 
 int launch_measure(swb_lattice *h, int accumulate)
@@ -412,6 +447,7 @@ int swb_create(swb_lattice **out, uint32_t L0, uint32_t L1, uint32_t tile_x, uin
     SWB_TRY(cudaMalloc(&h->rng_sel, (size_t)h->n_tiles * h->W));
     SWB_TRY(cudaMalloc(&h->rng_iter, (size_t)h->n_tiles * sizeof(uint32_t)));
     SWB_TRY(cudaMalloc(&h->edge, (size_t)h->n_blocks * kEdgeWords * sizeof(uint32_t)));
+    SWB_TRY(cudaMalloc(&h->linked, (size_t)h->n_blocks * (h->g.BX + h->g.BY) * sizeof(uint32_t)));
     SWB_TRY(cudaMalloc(&h->obs, sizeof(Obs)));
     h->series_cap = 1ull << 17;  // 131072 measurements (2 MiB)
     SWB_TRY(cudaMalloc(&h->series, h->series_cap * 2 * sizeof(long long)));
@@ -449,6 +485,7 @@ int swb_destroy(swb_lattice *h)
     cudaFree(h->rng_sel);
     cudaFree(h->rng_iter);
     cudaFree(h->edge);
+    cudaFree(h->linked);
     cudaFree(h->obs);
     cudaFree(h->series);
     cudaFree(h->scratch_flag);
@@ -694,7 +731,7 @@ int swb_launches_per_sweep(swb_lattice *h, uint32_t *launches)
 {
     if (!h || !launches)
         return fail(SWB_ERR_ARGUMENT, "NULL argument");
-    *launches = 3;
+    *launches = h->linked ? 4 : 3;
     return SWB_OK;
 }
 
@@ -722,11 +759,18 @@ int swb_sweep_timed(swb_lattice *h, float temperature, uint32_t n_sweeps, int pe
         if ((rc = launch_assign(h, p_add, nullptr, nullptr)))
             break;
         SWB_CUDA(cudaEventRecord(ev[2], h->stream));
-        k_merge<<<dim3(h->g.nbx, h->g.nby), h->g.BX + h->g.BY, 0, h->stream>>>(h->g, h->edge, h->labels, h->fault);
+        k_merge<<<dim3(h->g.nbx, h->g.nby), h->g.BX + h->g.BY, 0, h->stream>>>(h->g, h->edge, h->labels, h->fault,
+                                                                               h->linked);
         SWB_LAUNCHED();
         SWB_CUDA(cudaEventRecord(ev[3], h->stream));
-        k_flip<false><<<dim3(h->g.nbx, h->g.nby), kFlipThreads, h->smem_flip, h->stream>>>(h->g, h->spins, h->labels, h->fault);
-        SWB_LAUNCHED();
+        // resolve + flip: the reference's ResolveLabels and FlipClusters
+        if (h->linked) {
+            k_resolve<<<dim3(h->g.nbx, h->g.nby), h->g.BX + h->g.BY, 0, h->stream>>>(h->g, h->linked, h->labels,
+                                                                                     h->fault);
+            SWB_LAUNCHED();
+        }
+        if ((rc = launch_flip(h, false)))
+            break;
         SWB_CUDA(cudaEventRecord(ev[4], h->stream));
         SWB_CUDA(cudaEventSynchronize(ev[4]));
         float t;

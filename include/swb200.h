@@ -133,8 +133,8 @@ int swb_device_buffers(swb_lattice *h, void **spins, void **labels);
 int swb_launches_per_sweep(swb_lattice *h, uint32_t *launches);
 
 /* n_sweeps sweeps like swb_sweep (no measurement), timed with CUDA events on the handle's
- * stream.  ms[0] = total elapsed; when per_kernel != 0 an event pair brackets every launch
- * and ms[1..3] = summed durations of the assign, merge and flip kernels.  Synchronous. */
+ * stream.  ms[0] = total elapsed; when per_kernel != 0 events bracket every phase and
+ * ms[1..3] = summed durations of the assign, merge and resolve + flip kernels.  Synchronous. */
 int swb_sweep_timed(swb_lattice *h, float temperature, uint32_t n_sweeps, int per_kernel, float *ms);
 
 /* Page-locked host memory for fast host<->device copies (cudaHostAlloc / cudaFreeHost). */
@@ -225,7 +225,8 @@ int swb_batch_sweep(swb_batch *b, uint32_t n_rounds, int measure);
 int swb_batch_synchronize(swb_batch *b);
 
 /* Like swb_batch_sweep without measurement, timed with CUDA events: ms[0] total; with
- * per_kernel, ms[1..3] = assign, merge, flip kernel time summed over rounds.  Synchronous. */
+ * per_kernel, ms[1..3] = assign, merge, resolve + flip kernel time summed over rounds.
+ * Synchronous. */
 int swb_batch_sweep_timed(swb_batch *b, uint32_t n_rounds, int per_kernel, float *ms);
 
 /* Per-lattice observables, as swb_accumulators / swb_samples. */
