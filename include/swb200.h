@@ -53,7 +53,11 @@ uint64_t swb_kernel_launches(void);
  * SwendsenWang_2D::Initialize (ising/src/swendsen_wang.cpp:148-199): extents must be
  * even (:154-155); at most 2^31 - 1 sites (labels are uint32, swendsen_wang.hpp:29-30, with
  * the top bit used internally).  tile_x in {8, 16, 32},
- * 2 <= tile_y <= 32, lcg_width in {8, 16, 32}.  Spins start all 0. */
+ * 2 <= tile_y <= 32, lcg_width in {8, 16, 32}.  Spins start all 0.  A lattice of full
+ * 128 x 32-site blocks, or of at least 4096 blocks, resolves merged roots in a kernel of
+ * their own before the flip, others in the flip; the environment variable
+ * SWB_RESOLVE_MIN_BLOCKS, read here, replaces that rule by a block count.  Both forms give
+ * identical results. */
 int swb_create(swb_lattice **out, uint32_t L0, uint32_t L1, uint32_t tile_x, uint32_t tile_y,
                uint32_t lcg_width, uint32_t seed_base, int device);
 

@@ -108,6 +108,16 @@ def test_sweeps_bit_exact_vs_oracle(gpu, oracle, L0, L1, tile, W, T, sweeps):
         assert sw.energy_magnetization_sums() == (e, m)
 
 
+@pytest.mark.parametrize("resolve_min", ["1", "1000000000"])
+@pytest.mark.parametrize("L0,L1,tile,W,T,sweeps", [CASES[0], CASES[3], CASES[4], CASES[7]])
+def test_resolve_kernel_and_chasing_flip_agree_with_oracle(gpu, oracle, monkeypatch, resolve_min, L0, L1, tile, W, T,
+                                                          sweeps):
+    """Merged roots resolved by their own kernel (threshold 1 block) or chased by the flip
+    (threshold above any lattice): both bit-exact with the oracle, stage dumps included."""
+    monkeypatch.setenv("SWB_RESOLVE_MIN_BLOCKS", resolve_min)
+    test_sweeps_bit_exact_vs_oracle(gpu, oracle, L0, L1, tile, W, T, sweeps)
+
+
 def test_set_rng_roundtrip_and_continue(gpu, oracle):
     L0 = L1 = 256
     spins = oracle.hot_start(L0, L1, 1)
