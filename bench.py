@@ -400,8 +400,8 @@ def build_mix(cp, device: int, lcg_width: int = 16):
 
 
 def plain_loop(cp, mix, tiles, steps: int, device: int) -> dict:
-    """The same mix swept by looping the single-lattice path (three launches per lattice per
-    sweep, each lattice on its own stream)."""
+    """The same mix swept by looping the single-lattice path (three or four launches per
+    lattice per sweep, each lattice on its own stream)."""
     handles = []
     for (L, T, seed), (tile, _) in zip(mix, tiles):
         h = cp.SwendsenWang2D(L, L, tile, 16, seed_base=seed, device=device)

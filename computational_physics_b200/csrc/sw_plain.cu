@@ -1,7 +1,7 @@
 // Swendsen-Wang sweep for the 2D Ising model on one B200 (sm_100a), behind the C ABI of
 // include/swb200.h.
 //
-// One sweep = three kernels on the handle's stream (reference phases in brackets,
+// One sweep = four kernels on the handle's stream (reference phases in brackets,
 // ising/src/swendsen_wang.cpp:201-219):
 //
 //   k_assign  [AssignLabels + the in-block part of MergeLabels]  one CTA per block of
@@ -19,8 +19,9 @@
 //   k_resolve [ResolveLabels]  every linked root's chain is walked once to the root (the
 //             cluster's minimum site index), which becomes its label.
 //   k_flip    [ResolveLabels + FlipClusters]  every site reads its block root's label;
-//             spin ^= root & 1.  (The static-scratch entry point has no room for the linked
-//             roots: its k_flip walks the merged roots' chains itself, without k_resolve.)
+//             spin ^= root & 1.  (Without k_resolve, three kernels, k_flip walks the merged
+//             roots' chains itself: small lattices of 128 x 16 blocks, see kResolveMinBlocks,
+//             and the static-scratch entry point, which has no room for the linked roots.)
 //
 // k_measure (every measure_every-th sweep) reduces energy and magnetisation on the device
 // and accumulates E, E^2, |M| in FP64 (Lattice<2>::GetEnergyAndMagnetization,
