@@ -20,7 +20,7 @@
 //             cluster's minimum site index), which becomes its label.
 //   k_flip    [ResolveLabels + FlipClusters]  every site reads its block root's label;
 //             spin ^= root & 1.  (Without k_resolve, three kernels, k_flip walks the merged
-//             roots' chains itself: small lattices of 128 x 16 blocks, see kResolveMinBlocks,
+//             roots' chains itself: small lattices of blocks under 128 x 32 sites, see kResolveMinBlocks,
 //             and the static-scratch entry point, which has no room for the linked roots.)
 //
 // k_measure (every measure_every-th sweep) reduces energy and magnetisation on the device
