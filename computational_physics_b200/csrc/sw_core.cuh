@@ -285,13 +285,15 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
     // Scanline labelling.  Work item = (32-column strip, band of rows); a warp walks its band
     // top-down with each lane holding the provisional label of the site above.  A run (x-bonded
     // sites of the strip row; its first lane from the gap mask below the lane) takes the label
-    // above its leftmost y-bonded site, or with none its own first site as a new label.  Every other y-bond of the run that meets a different label unites the
-    // two in the shared union-find (toward the minimum), so each site's root is the minimum of
-    // its block-local component.  Seams between strips and bands are united afterwards, then
-    // every site resolves its provisional label.
+    // above its leftmost y-bonded site, or with none its own first site as a new label.  Every
+    // other y-bond of the run that meets a different label unites the two in the shared
+    // union-find (toward the minimum), so each site's root is the minimum of its block-local
+    // component.  Seams between strips and bands are united afterwards, then every site
+    // resolves its provisional label.
     uint16_t *plab = reinterpret_cast<uint16_t *>(smem + L.plab);
     const uint32_t nb = max(1u, nwarps >> lnw);              // bands
-    const uint32_t rb = (nb & (nb - 1)) == 0 ? (BY + nb - 1) >> (__ffs(nb) - 1) : (BY + nb - 1) / nb;  // rows per band
+    const uint32_t rb = (nb & (nb - 1)) == 0 ? (BY + nb - 1) >> (__ffs(nb) - 1)  // rows per band
+                                             : (BY + nb - 1) / nb;
     const uint32_t below = (1u << lane) - 1u;                // lanes below this one
     for (uint32_t task = warp; task < NW * nb; task += nwarps) {
         const uint32_t sx = task & (NW - 1), band = task >> lnw;
