@@ -125,3 +125,13 @@ def test_latency_summary():
     assert s["makespan_s"] == pytest.approx(7.0)
     assert s["site_updates_per_s"] == pytest.approx(4 * 32 * 32 * 100 / 7.0)
     assert serving.latency_summary([serving.Job(0, 32, 2.0, 1, 1)]) == {"jobs": 0}
+
+
+def test_autotune_choice_uses_the_nearest_tuned_side():
+    from computational_physics_b200 import autotune
+    table = autotune.load("NVIDIA B200")
+    assert autotune.choice(64, table) == ((16, 4), (4, 8))       # the committed B200 table's entry for 64
+    assert autotune.choice(70, table) == autotune.choice(64, table)
+    assert autotune.choice(4096, table) == autotune.choice(512, table)
+    assert autotune.choice(100, {}) == ((16, 8), (0, 0))          # no table: the default tile
+    assert autotune.cache_path("NVIDIA B200", 16).endswith("tuned/nvidia_b200_w16.json")
