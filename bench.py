@@ -57,6 +57,8 @@ def mix_workload(count: int = MIX_COUNT, seed: int = MIX_SEED):
 
 PLAIN = {
     "plain16384": dict(L=16384, tile=(16, 8), W=16, T=T_C),
+    "plain8192": dict(L=8192, tile=(16, 8), W=16, T=T_C),
+    "plain4096": dict(L=4096, tile=(16, 8), W=16, T=T_C),
     "plain1024": dict(L=1024, tile=(8, 8), W=16, T=T_C),
 }
 
@@ -111,16 +113,63 @@ class Dist:
 # clocks during the timed region
 
 class ClockSampler:
+    """SM clock and clock-event reasons of one GPU, sampled every 10 ms by NVML (read-only
+    queries) from a thread while the timed region runs, plus one sample as it ends, so that even
+    a region of a few milliseconds has samples.  Falls back to nvidia-smi (every 200 ms) when
+    NVML is unavailable."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20, "sw_power_cap": 0x4}
 
-    def __init__(self, device: int):
+    def __init__(self, device: int, period_s: float = 0.01):
         self.device = device
+        self.period = period_s
         self.proc = None
+        self.nvml = None
+        self.handle = None
+        self.stop = threading.Event()
         self.lines: list[str] = []
 
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        self.nvml = pynvml
+        try:  # the CUDA device by UUID (NVML numbers every GPU of the host, CUDA only the visible ones)
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.device).uuid)
+            return pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return pynvml.nvmlDeviceGetHandleByIndex(self.device)
+
+    def _nvml_sample(self):
+        n, h = self.nvml, self.handle
+        sm = n.nvmlDeviceGetClockInfo(h, n.NVML_CLOCK_SM)
+        mx = n.nvmlDeviceGetMaxClockInfo(h, n.NVML_CLOCK_SM)
+        get = getattr(n, "nvmlDeviceGetCurrentClocksEventReasons", None) or n.nvmlDeviceGetCurrentClocksThrottleReasons
+        r = get(h)
+        flags = ["Active" if r & bit else "Not Active" for bit in self.REASONS.values()]
+        self.lines.append(",".join([str(self.device), str(sm), str(mx), "", hex(r), *flags]))
+
+    def _poll(self):
+        while not self.stop.is_set():
+            try:
+                self._nvml_sample()
+            except Exception:
+                return
+            self.stop.wait(self.period)
+
     def __enter__(self):
+        try:
+            self.handle = self._nvml_handle()
+            self._nvml_sample()
+            self.lines.clear()
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
@@ -140,6 +189,13 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *exc):
+        if self.nvml is not None:
+            try:
+                self._nvml_sample()  # the end of the timed region
+            except Exception:
+                pass
+            self.stop.set()
+            self.thread.join(timeout=2)
         if self.proc:
             self.proc.terminate()
             try:
@@ -345,6 +401,8 @@ def bench_plain(args, dist: Dist, cp) -> dict:
                 flush.synchronize()
                 ms += float(sw.sweep_timed(T, 1)[0])
     launches = cp.kernel_launches() - launches0 - (0 if big else 2 * args.steps)
+    if flush is not None:
+        flush.close()
     dist.barrier()
     ms_max = dist.max(ms)
     value = dist.world * n * args.steps / (ms_max / 1e3)

@@ -5,7 +5,7 @@ Python host mirror of the reference's interface (flwende/computational_physics):
 * :class:`SwendsenWang2D` -- one lattice on one GPU, the drop-in for
   ``SwendsenWang_2D<LCG32, Target>::Update`` plus ``Lattice<2>``'s observables
   (ising/include/swendsen_wang.hpp:26-102, ising/include/lattice.hpp:21-95);
-* :func:`p_add` -- the bond probability exactly as ising/src/swendsen_wang.cpp:207.
+* :func:`p_add` -- the bond probability exactly as ising/src/swendsen_wang.cpp:100.
 
 Everything runs through the C ABI of ``include/swb200.h`` in ``lib/libswb200.so``
 (hand-written CUDA for sm_100a).  There is no CPU fallback: importing works without a

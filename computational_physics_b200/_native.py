@@ -45,6 +45,8 @@ _SIGNATURES = {
     "swb_accept_threshold": ([F32], U32),
     "swb_sweep": ([P, F32, U32, U32], I32),
     "swb_sweep_recorded": ([P, F32, P, P, P], I32),
+    "swb_sweep_dumped": ([P, F32, P, P, P], I32),
+    "swb_geometry": ([P, P], I32),
     "swb_synchronize": ([P], I32),
     "swb_energy_magnetization": ([P, P, P, P], I32),
     "swb_accumulators": ([P, P], I32),
@@ -57,6 +59,14 @@ _SIGNATURES = {
     "swb_launches_per_sweep": ([P, P], I32),
     "swb_update_host": ([P, F32, P, P, P], I32),
     "swb_sweep_timed": ([P, F32, U32, I32, P], I32),
+    "swb_attach_spins": ([P, P], I32),
+    "swb_device_alloc": ([I32, ctypes.c_size_t, P], I32),
+    "swb_device_free": ([I32, P], I32),
+    "swb_copy_to_device": ([I32, P, P, ctypes.c_size_t], I32),
+    "swb_copy_to_host": ([I32, P, P, ctypes.c_size_t], I32),
+    "swb_device_synchronize": ([I32], I32),
+    "swb_device_sm_count": ([I32, P], I32),
+    "swb_spins_energy_magnetization": ([I32, U32, U32, P, P, P, P], I32),
     "swb_host_alloc": ([P, ctypes.c_size_t], I32),
     "swb_host_free": ([P], I32),
     "swb_sweep_static": ([P, U32, U32, U32, U32, U32, F32, U32, P, P, P, P, I32], I32),

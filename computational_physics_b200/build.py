@@ -1,7 +1,9 @@
 """Builds the native libraries of the package in-tree.
 
   computational_physics_b200/lib/libswb200.so   CUDA kernels + C ABI (include/swb200.h), sm_100a
-  computational_physics_b200/lib/Ising2D        the Ising2D command line program (nvidia_gpu target)
+
+The reference's own Ising2D program with the nvidia_gpu target is built from the reference
+sources by computational_physics_b200/dropin/build_dropin.py (into lib/dropin/).
 
 Usage: python -m computational_physics_b200.build [--verbose]
 """
@@ -16,7 +18,6 @@ import sys
 PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
-HOST = os.path.join(PKG, "host")
 LIB = os.path.join(PKG, "lib")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
@@ -51,13 +52,6 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
     if force or _stale(so, deps):
         extra = ["-Xptxas", "-v"] if ptxas_info else []
         _run([nvcc(), *ARCH, *NVCC_FLAGS, *extra, "-shared", "-o", so, *cu, "-lcudart"], verbose)
-    host_src = sorted(glob.glob(os.path.join(HOST, "*.cpp")))
-    host_hdr = sorted(glob.glob(os.path.join(HOST, "*.hpp")))
-    exe = os.path.join(LIB, "Ising2D")
-    if host_src and (force or _stale(exe, host_src + host_hdr + [so])):
-        _run(["/usr/bin/g++", "-std=c++20", "-O2", "-Wall", "-I", os.path.join(ROOT, "include"), "-I", HOST,
-              "-o", exe, *host_src, "-L", LIB, "-lswb200", f"-Wl,-rpath,{LIB}", "-Wl,-rpath,$ORIGIN",
-              "-lpthread"], verbose)
     return so
 
 

@@ -22,6 +22,13 @@ extern thread_local std::string g_last_error;
 extern std::atomic<uint64_t> g_launches;
 int fail(int code, const char *fmt, ...);
 
+// swb_sweep_static's scratch: one file-scope device array (sw_static_scratch.cu) holding the
+// label array, the block edge words and the fault word of a lattice of at most 2048 x 2048 sites.
+constexpr uint64_t kStaticMaxSites = 1ull << 22;               // 2048 x 2048 sites
+constexpr size_t kStaticScratchBytes = (24ull << 20) + 1024;   // labels 16 MiB + edge words + fault
+// Device address of that array on `device`, which must be current (looked up once per device).
+int static_scratch_base(int device, unsigned char **base);
+
 #define SWB_CUDA(call)                                                                          \
     do {                                                                                        \
         cudaError_t err__ = (call);                                                             \
@@ -97,6 +104,7 @@ struct U32 {  // a compile-time uint32_t passed as a value
 
 constexpr uint32_t kMaxGridY = 65535;  // block rows of a lattice: the kernels' grid y
 constexpr uint32_t kEdgeWords = 8;  // per block: [0] right edge rows, [1..4] bottom edge columns
+constexpr uint32_t kEdgeE = 6, kEdgeM = 7;  // shared-memory copies of words 6, 7: the block's energy / magnetisation sums
 
 // Label encoding between the assign and flip phases of a sweep.  A block root holds its global
 // site index (< 2^31); these are the only entries the merge reads and links.  Every other site
@@ -116,6 +124,74 @@ __device__ __forceinline__ uint32_t label_global(const Geo &g, uint32_t bxi, uin
     const uint32_t yl = (g.BX & (g.BX - 1)) == 0 ? r >> (__ffs(g.BX) - 1) : r / g.BX;
     return (byi * g.BY + yl) * g.L0 + bxi * g.BX + (r - yl * g.BX);
 }
+
+// Observables.  Per-sweep integer sums land in obs->e / obs->m; the last CTA turns them into
+// E/N, M/N, accumulates E, E^2, |M| in FP64 and appends (e, m) to the sample series.
+struct Obs {
+    unsigned long long e, m;       // running int64 sums (two's complement) of this measurement
+    unsigned int done;             // CTAs finished
+    unsigned int pad;
+    long long last_e, last_m;      // sums of the last measurement
+    double acc[4];                 // sum E/N, sum (E/N)^2, sum |M/N|, samples
+    unsigned long long n_samples;  // samples recorded (may exceed capacity)
+};
+
+// One part of a measurement: adds this part's integer sums (e = sum s (s_right + s_down),
+// m = sum s over its sites) and, if it is the last of n_parts, turns the totals into E/N and
+// M/N, accumulates E, E^2, |M| in FP64 (with accumulate), appends (e, m) to the series and
+// clears the sums for the next measurement.  Called by one thread per part.
+__device__ __forceinline__ void obs_add_part(Obs *obs, long long *series, const unsigned long long cap, const size_t n,
+                                             const unsigned int n_parts, const long long e, const long long m,
+                                             const int accumulate)
+{
+    atomicAdd(&obs->e, (unsigned long long)e);
+    atomicAdd(&obs->m, (unsigned long long)m);
+    __threadfence();
+    const unsigned int ticket = atomicAdd(&obs->done, 1u);
+    if (ticket == n_parts - 1) {
+        __threadfence();
+        const long long te = (long long)atomicAdd(&obs->e, 0ull);
+        const long long tm = (long long)atomicAdd(&obs->m, 0ull);
+        obs->last_e = te;
+        obs->last_m = tm;
+        if (accumulate) {
+            const double E = -(double)te / (double)n, M = (double)tm / (double)n;
+            obs->acc[0] += E;
+            obs->acc[1] += E * E;
+            obs->acc[2] += fabs(M);
+            obs->acc[3] += 1.0;
+            const unsigned long long k = obs->n_samples;
+            if (k < cap) {
+                series[2 * k] = te;
+                series[2 * k + 1] = tm;
+            }
+            obs->n_samples = k + 1;
+        }
+        obs->e = 0;
+        obs->m = 0;
+        obs->done = 0;
+    }
+}
+
+// A measurement of the spins a sweep starts from, made by its assign phase (obs null: none).
+// The blocks of the sweep are its parts.
+struct MeasureArgs {
+    Obs *obs;
+    long long *series;
+    unsigned long long cap;
+};
+
+// Optional dumps of the assign phase to device buffers (one entry per site, row-major).  All
+// null in a plain sweep; set by the recording entry points.  bonds: bit 0 +x, bit 1 +y (every
+// bond of the sweep, block edges and the periodic wrap included); block_labels: the minimum
+// global site index of the site's component over the bonds inside its block (the labels the
+// assign phase hands to the merge); tile_labels: the same inside the site's tile (the
+// reference's AssignLabels stage), which only the tile-by-tile form below computes.
+struct AssignDump {
+    uint8_t *bonds;
+    uint32_t *block_labels;
+    uint32_t *tile_labels;
+};
 
 struct AssignSmem {
     uint32_t parent, draws, slots, edge, bond, sp, plab, total, pitch;
@@ -206,31 +282,27 @@ __device__ __forceinline__ uint32_t spin_bits32(const uint8_t *p)
 // accepted draws in shared memory: bond bitmasks per 32-site word, then a scanline pass over
 // x-runs (below).  The result equals the generic path's: the minimum site index of each
 // block-local component.
+// Bond words of block (bxi, byi) into shared memory: Xw / Yw [BY][NW] hold the x- and y-bonds
+// inside the block, edge_s the bonds that leave it through its last column (word 0, one bit
+// per row) and its last row (words 1..NW).  Needs the staged spins and the draw words.
 template <int W, int TXc, int TYc>
-__device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uint32_t bxi, const uint32_t byi,
-                                                         uint32_t *__restrict__ labels, uint32_t *__restrict__ edge,
-                                                         unsigned char *smem)
+__device__ __forceinline__ void block_bond_words(const Geo &g, const uint32_t bxi, const uint32_t byi,
+                                                 const bool measure, const AssignSmem &L, unsigned char *smem)
 {
-    const AssignSmem L = assign_smem(g, W);
     const uint32_t TX = TXc ? TXc : g.TX, TY = TYc ? TYc : g.TY;  // compile-time for the common tiles
     const uint32_t Ur = (TX + W - 1) / W, um = (2 * TY - 1) * Ur;  // updates per row request; merge request
-    uint32_t *parent = reinterpret_cast<uint32_t *>(smem + L.parent);
     const DrawWords<W> dw{reinterpret_cast<const uint32_t *>(smem + L.draws), L.slots};
     uint32_t *edge_s = reinterpret_cast<uint32_t *>(smem + L.edge);
     const uint8_t *sp = smem + L.sp;
     const uint32_t BX = g.BX, BY = g.BY, NW = BX >> 5, lnw = __ffs(NW) - 1;  // NW is a power of two
-    uint32_t *Xw = reinterpret_cast<uint32_t *>(smem + L.bond);  // [BY][NW] x-bonds inside the block
-    uint32_t *Yw = Xw + BY * NW;                                  // [BY][NW] y-bonds inside the block
-    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    uint32_t *Xw = reinterpret_cast<uint32_t *>(smem + L.bond);
+    uint32_t *Yw = Xw + BY * NW;
+    const uint32_t tid = threadIdx.x;
     const uint32_t x0 = bxi * BX, y0 = byi * BY;
     const uint32_t bxv = min(BX, g.L0 - x0), byv = min(BY, g.L1 - y0);
     const uint32_t pitch = L.pitch;
     const uint32_t txs = TXc ? (TXc == 8 ? 3 : TXc == 16 ? 4 : 5) : 31 - __clz(TX);  // TX is 8, 16 or 32
-
-    // Every site starts as its own root (16-byte stores; parent is at offset 0 and BX*BY is a
-    // multiple of 64).
-    for (uint32_t i = tid; i < (BX * BY) >> 2; i += blockDim.x)
-        reinterpret_cast<uint4 *>(parent)[i] = make_uint4(4 * i, 4 * i + 1, 4 * i + 2, 4 * i + 3);
+    (void)x0; (void)y0;
 
     // Bond words, bit-parallel: one thread per 32-site word of a row.  Spin bits come from the
     // staged bytes (the word, the word below and the byte to its right: the halo column and
@@ -239,6 +311,7 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
     // column from the merge request's right edge (bit TX + jj); y bonds from the row's y request,
     // or on the tile's last row from the merge request's bottom edge (bits [0, TX)).  Edge bonds
     // go to edge_s (right edge: one bit per row, bottom: the row's words).
+    int esum = 0, msum = 0;  // energy / magnetisation of this thread's words (the spins before the flip)
     for (uint32_t i = tid; i < BY * NW; i += blockDim.x) {
         const uint32_t yl = i >> lnw, w = i & (NW - 1);
         uint32_t X = 0, Y = 0;
@@ -266,6 +339,12 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
             }
             X = ~(S ^ R) & AX;
             Y = ~(S ^ D) & AY;
+            {   // s (s_right + s_down) and s over the word's sites: +1 per equal pair, -1 per unequal one
+                const uint32_t nv = min(32u, bxv > (w << 5) ? bxv - (w << 5) : 0u);
+                const uint32_t vm = nv == 32 ? 0xFFFFFFFFu : (1u << nv) - 1u;
+                esum += 2 * (int)nv - 2 * (__popc((S ^ R) & vm) + __popc((S ^ D) & vm));
+                msum += 2 * __popc(S & vm) - (int)nv;
+            }
             if (bxv - 1 - (w << 5) < 32u) {  // the block's last column lies in this word
                 const uint32_t bit = (bxv - 1) & 31;
                 if ((X >> bit) & 1u)
@@ -280,6 +359,63 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
         Xw[yl * NW + w] = X;
         Yw[yl * NW + w] = Y;
     }
+    if (measure) {  // warp sums into the block's two shared words (zeroed with the edge words)
+        esum = __reduce_add_sync(0xffffffffu, esum);
+        msum = __reduce_add_sync(0xffffffffu, msum);
+        if ((tid & 31) == 0 && (tid >> 5) < ((BY * NW + 31) >> 5)) {
+            atomicAdd(reinterpret_cast<int *>(edge_s + kEdgeE), esum);
+            atomicAdd(reinterpret_cast<int *>(edge_s + kEdgeM), msum);
+        }
+    }
+}
+
+// Recording only (after the block's labels are stored and its CTA synchronised): every bond of
+// the block's sites, and each site's block-local component as a global site index.
+template <int W>
+__device__ __forceinline__ void dump_block(const Geo &g, const uint32_t bxi, const uint32_t byi,
+                                        const uint32_t *labels, const AssignDump &dump, unsigned char *smem)
+{
+    const AssignSmem L = assign_smem(g, W);
+    const uint32_t *edge_s = reinterpret_cast<const uint32_t *>(smem + L.edge);
+    const uint32_t BX = g.BX, BY = g.BY, NW = BX >> 5;
+    const uint32_t *Xw = reinterpret_cast<const uint32_t *>(smem + L.bond), *Yw = Xw + BY * NW;
+    const uint32_t x0 = bxi * BX, y0 = byi * BY;
+    const uint32_t bxv = min(BX, g.L0 - x0), byv = min(BY, g.L1 - y0);
+    for (uint32_t i = threadIdx.x; i < bxv * byv; i += blockDim.x) {
+        const uint32_t yl = i / bxv, xl = i - yl * bxv, w = xl >> 5, k = xl & 31;
+        const size_t site = (size_t)(y0 + yl) * g.L0 + x0 + xl;
+        if (dump.bonds) {
+            const uint32_t xb = xl + 1 == bxv ? (edge_s[0] >> yl) & 1u : (Xw[yl * NW + w] >> k) & 1u;
+            const uint32_t yb = yl + 1 == byv ? (edge_s[1 + w] >> k) & 1u : (Yw[yl * NW + w] >> k) & 1u;
+            dump.bonds[site] = (uint8_t)(xb | yb << 1);
+        }
+        if (dump.block_labels)
+            dump.block_labels[site] = label_global(g, bxi, byi, labels[site]);
+    }
+}
+
+template <int W, int TXc, int TYc, bool kMayDump>
+__device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uint32_t bxi, const uint32_t byi,
+                                                         uint32_t *__restrict__ labels, uint32_t *__restrict__ edge,
+                                                         const AssignDump &dump, const MeasureArgs &meas,
+                                                         unsigned char *smem)
+{
+    const AssignSmem L = assign_smem(g, W);
+    uint32_t *parent = reinterpret_cast<uint32_t *>(smem + L.parent);
+    uint32_t *edge_s = reinterpret_cast<uint32_t *>(smem + L.edge);
+    const uint32_t BX = g.BX, BY = g.BY, NW = BX >> 5, lnw = __ffs(NW) - 1;  // NW is a power of two
+    uint32_t *Xw = reinterpret_cast<uint32_t *>(smem + L.bond);  // [BY][NW] x-bonds inside the block
+    uint32_t *Yw = Xw + BY * NW;                                  // [BY][NW] y-bonds inside the block
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    const uint32_t x0 = bxi * BX, y0 = byi * BY;
+    const uint32_t bxv = min(BX, g.L0 - x0), byv = min(BY, g.L1 - y0);
+
+    // Every site starts as its own root (16-byte stores; parent is at offset 0 and BX*BY is a
+    // multiple of 64).
+    for (uint32_t i = tid; i < (BX * BY) >> 2; i += blockDim.x)
+        reinterpret_cast<uint4 *>(parent)[i] = make_uint4(4 * i, 4 * i + 1, 4 * i + 2, 4 * i + 3);
+
+    block_bond_words<W, TXc, TYc>(g, bxi, byi, meas.obs != nullptr, L, smem);
     __syncthreads();
 
     // Scanline labelling.  Work item = (32-column strip, band of rows); a warp walks its band
@@ -389,6 +525,13 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
     }
     if (tid < kEdgeWords)
         edge[((size_t)byi * g.nbx + bxi) * kEdgeWords + tid] = edge_s[tid];
+    if (meas.obs && tid == 0)  // the block's sums (complete since the barrier after the bond words)
+        obs_add_part(meas.obs, meas.series, meas.cap, (size_t)g.L0 * g.L1, g.nbx * g.nby,
+                     reinterpret_cast<const int *>(edge_s)[kEdgeE], reinterpret_cast<const int *>(edge_s)[kEdgeM], 1);
+    if (kMayDump && (dump.bonds || dump.block_labels)) {  // recording only
+        __syncthreads();
+        dump_block<W>(g, bxi, byi, labels, dump, smem);
+    }
 }
 
 // Block (bxi, byi) of a lattice: lcg32 draws, bonds, union-find in shared memory.  Runs on
@@ -396,13 +539,13 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
 // kPhaseSeq selects the phase-dispatched draw sequence (below) for full-height tiles of a
 // compile-time shape: on B200 it is the faster form inside the batched kernel (whose item loop
 // keeps more registers live) and the slower one in the single-lattice kernel.
-template <int W, int TXc = 0, int TYc = 0, bool kPhaseSeq = false>
+template <int W, int TXc = 0, int TYc = 0, bool kPhaseSeq = false, bool kMayDump = true>
 __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, const uint32_t byi,
                                              const uint8_t *__restrict__ spins, uint32_t *__restrict__ labels,
                                              uint32_t *__restrict__ rng_state, uint8_t *__restrict__ rng_sel,
                                              uint32_t *__restrict__ rng_iter, const uint32_t thr,
-                                             uint32_t *__restrict__ edge, uint8_t *__restrict__ dbg_bonds,
-                                             uint32_t *__restrict__ dbg_assign, unsigned char *smem)
+                                             uint32_t *__restrict__ edge, const AssignDump dump,
+                                             const MeasureArgs meas, unsigned char *smem)
 {
     const AssignSmem L = assign_smem(g, W);
     const uint32_t TX = TXc ? TXc : g.TX, TY = TYc ? TYc : g.TY;  // compile-time for the common tiles
@@ -490,7 +633,7 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
             it = rng_iter[tile];
         }
         uint32_t a = lcg_param_a(sel), c = lcg_param_c(sel);
-        // The parameter rotation of LCG32_State::Update (random/src/lcg32.cpp:162-195): before
+        // The parameter rotation of LCG32_State::Update (random/src/lcg32.cpp:51-84): before
         // update itn when itn is a multiple of 15, the (a, c) pairs rotate by
         // state[itn & (W-1)] + (itn odd ? 0 : 1).
         auto rotate = [&](const uint32_t itn, const bool rot) {
@@ -615,8 +758,8 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
         sp[tid * pitch + bxv] = halo;
     __syncthreads();
 
-    if (dbg_assign == nullptr && (BX & 31u) == 0 && (BX & (BX - 1)) == 0) {
-        assign_block_labels_rows<W, TXc, TYc>(g, bxi, byi, labels, edge, smem);
+    if (dump.tile_labels == nullptr && (BX & 31u) == 0 && (BX & (BX - 1)) == 0) {
+        assign_block_labels_rows<W, TXc, TYc, kMayDump>(g, bxi, byi, labels, edge, dump, meas, smem);
         return;
     }
 
@@ -656,14 +799,17 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
             uf_union(parent, l, l + BX);
     }
     __syncthreads();
-    if (dbg_assign != nullptr) {
+    if (kMayDump && (dump.bonds || dump.tile_labels)) {  // recording only
         for (uint32_t l = tid; l < NS; l += nthr) {
             const uint32_t xl = l % BX, yl = l / BX;
             if (xl < bxv && yl < byv) {
-                const uint32_t r = uf_find(parent, l);
                 const size_t site = (size_t)(y0 + yl) * g.L0 + x0 + xl;
-                dbg_assign[site] = (y0 + r / BX) * g.L0 + x0 + r % BX;
-                dbg_bonds[site] = bond[l];
+                if (dump.tile_labels) {
+                    const uint32_t r = uf_find(parent, l);
+                    dump.tile_labels[site] = (y0 + r / BX) * g.L0 + x0 + r % BX;
+                }
+                if (dump.bonds)
+                    dump.bonds[site] = bond[l];
             }
         }
         __syncthreads();
@@ -700,6 +846,8 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
         if (xl < bxv && yl < byv) {
             const uint32_t r = uf_find(parent, l);
             labels[(size_t)(y0 + yl) * g.L0 + x0 + xl] = r == l ? (y0 + yl) * g.L0 + x0 + xl : (kLocalFlag | r);
+            if (kMayDump && dump.block_labels)  // recording only
+                dump.block_labels[(size_t)(y0 + yl) * g.L0 + x0 + xl] = (y0 + r / BX) * g.L0 + x0 + r % BX;
         }
     }
     if (tid < kEdgeWords)
@@ -717,8 +865,8 @@ __device__ __forceinline__ void assign_block_any(const Geo &g, const uint32_t bx
 {
 #define SWB_TILE(tx, ty)                                                                                              \
     if (g.TX == tx && g.TY == ty) {                                                                                   \
-        assign_block<W, tx, ty, true>(g, bxi, byi, spins, labels, rng_state, rng_sel, rng_iter, thr, edge, nullptr, \
-                                      nullptr, smem);                                                                 \
+        assign_block<W, tx, ty, true, false>(g, bxi, byi, spins, labels, rng_state, rng_sel, rng_iter, thr, edge,   \
+                                             AssignDump{}, MeasureArgs{}, smem);                                      \
         return;                                                                                                       \
     }
     if constexpr (W == 16) {
@@ -731,7 +879,8 @@ __device__ __forceinline__ void assign_block_any(const Geo &g, const uint32_t bx
         SWB_TILE(16, 4)
     }
 #undef SWB_TILE
-    assign_block<W>(g, bxi, byi, spins, labels, rng_state, rng_sel, rng_iter, thr, edge, nullptr, nullptr, smem);
+    assign_block<W, 0, 0, false, false>(g, bxi, byi, spins, labels, rng_state, rng_sel, rng_iter, thr, edge,
+                                        AssignDump{}, MeasureArgs{}, smem);
 }
 
 // Unions across the right and bottom edge (periodic) of block (bxi, byi): thread t < BY takes
@@ -901,15 +1050,5 @@ __device__ __forceinline__ void flip_block(const Geo &g, const uint32_t bxi, con
     }
 }
 
-// Observables.  Per-sweep integer sums land in obs->e / obs->m; the last CTA turns them into
-// E/N, M/N, accumulates E, E^2, |M| in FP64 and appends (e, m) to the sample series.
-struct Obs {
-    unsigned long long e, m;       // running int64 sums (two's complement) of this measurement
-    unsigned int done;             // CTAs finished
-    unsigned int pad;
-    long long last_e, last_m;      // sums of the last measurement
-    double acc[4];                 // sum E/N, sum (E/N)^2, sum |M/N|, samples
-    unsigned long long n_samples;  // samples recorded (may exceed capacity)
-};
 
 }  // namespace swb

@@ -2,7 +2,7 @@
 //
 //  * lcg32 lanes in registers: one thread holds one lane of a tile's stream; a tile's W
 //    lanes sit in one W-wide segment of a warp, so the reference's periodic parameter
-//    rotation (random/src/lcg32.cpp:162-195) is a segment-local __shfl_sync.
+//    rotation (random/src/lcg32.cpp:51-84) is a segment-local __shfl_sync.
 //  * drand48 with jump-ahead, for the bit-exact hot start and stream seeding.
 //  * lock-free union-find toward the minimum index (shared or global memory), the
 //    reference's atomic-min equivalence rule (ising/src/swendsen_wang_cpu.cpp:107-156).
@@ -12,7 +12,7 @@
 
 namespace swb {
 
-// The five Numerical Recipes (a, c) pairs of random/src/lcg32.cpp:128-135, by index.
+// The five Numerical Recipes (a, c) pairs of random/src/lcg32.cpp:17-24, by index.
 __host__ __device__ __forceinline__ uint32_t lcg_param_a(uint32_t sel)
 {
     return sel == 0 ? 1372383749u : sel == 1 ? 2891336453u : sel == 2 ? 2024337845u : sel == 3 ? 32310901u : 29943829u;
@@ -35,7 +35,7 @@ constexpr uint32_t kShuffleDistance = 15;          // LCG32_State::ShuffleDistan
 constexpr float kTwoPowMinus32 = 2.3283064365386963e-10f;  // the float the reference's literal rounds to
 
 // Accept test of a bond draw.  The reference accepts when (float)u * 2^-32 < p_add, with u
-// rounded to nearest (random/src/lcg32.cpp:231-240 and the '< p_add' of its callers).  The
+// rounded to nearest (random/src/lcg32.cpp:120-129 and the '< p_add' of its callers).  The
 // scaling by 2^-32 is exact and round-to-nearest conversion is monotone in u, so the accepted
 // u are exactly the prefix [0, thr) with thr = accept_threshold(p_add): one integer compare.
 __device__ __forceinline__ bool lcg_accept(uint32_t u, uint32_t thr)

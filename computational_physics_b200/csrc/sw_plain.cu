@@ -2,7 +2,7 @@
 // include/swb200.h.
 //
 // One sweep = four kernels on the handle's stream (reference phases in brackets,
-// ising/src/swendsen_wang.cpp:201-219):
+// ising/src/swendsen_wang.cpp:94-112):
 //
 //   k_assign  [AssignLabels + the in-block part of MergeLabels]  one CTA per block of
 //             TBX x TBY tiles.  Each tile's lcg32 stream lives in the registers of one
@@ -25,7 +25,7 @@
 //
 // k_measure (every measure_every-th sweep) reduces energy and magnetisation on the device
 // and accumulates E, E^2, |M| in FP64 (Lattice<2>::GetEnergyAndMagnetization,
-// ising/src/lattice.cpp:127-165, and the sums of ising/src/ising_2d.cpp:127-146).
+// ising/src/lattice.cpp:29-67, and the sums of ising/src/ising_2d.cpp:127-146).
 //
 // Bit-exactness with the reference CPU path: the stream of tile t is seeded seed_base + t
 // and consumed in the reference's order (rows' x-draws, rows' y-draws, then the merge draw
@@ -34,6 +34,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdarg>
@@ -68,18 +69,21 @@ int fail(int code, const char *fmt, ...)
 
 constexpr uint32_t kAssignThreads = 512;  // at most this many lcg lanes per block
 
-// kDebug adds the stage dumps (bond bytes and tile-local labels) of a recorded sweep.  TXc, TYc
-// make the tile shape a compile-time constant for the common shapes (0 = runtime).
-template <int W, int TXc, int TYc, bool kDebug>
+// TXc, TYc make the tile shape a compile-time constant for the common shapes (0 = runtime).
+// `dump` is all null in a plain sweep; a recorded sweep runs the same instance with dumps on
+// (the tile-local stage only through the runtime-shape instance, which labels tile by tile).
+// kMeasure: the instance that also measures the spins it starts from (`meas`), used by the
+// sweep after a measured one; a separate instance so the others carry none of its registers.
+template <int W, int TXc, int TYc, bool kMeasure>
 __global__ void __launch_bounds__(kAssignThreads, 4) k_assign(const Geo g, const uint8_t *__restrict__ spins,
                                                  uint32_t *__restrict__ labels, uint32_t *__restrict__ rng_state,
                                                  uint8_t *__restrict__ rng_sel, uint32_t *__restrict__ rng_iter,
-                                                 const uint32_t thr, uint32_t *__restrict__ edge,
-                                                 uint8_t *__restrict__ dbg_bonds, uint32_t *__restrict__ dbg_assign)
+                                                 const uint32_t thr, uint32_t *__restrict__ edge, const AssignDump dump,
+                                                 const MeasureArgs meas)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    assign_block<W, TXc, TYc>(g, blockIdx.x, blockIdx.y, spins, labels, rng_state, rng_sel, rng_iter, thr, edge,
-                              kDebug ? dbg_bonds : nullptr, kDebug ? dbg_assign : nullptr, smem);
+    assign_block<W, TXc, TYc>(g, blockIdx.x, blockIdx.y, spins, labels, rng_state, rng_sel, rng_iter, thr, edge, dump,
+                              kMeasure ? meas : MeasureArgs{}, smem);
 }
 
 __global__ void __launch_bounds__(256) k_merge(const Geo g, const uint32_t *__restrict__ edge, uint32_t *labels,
@@ -146,37 +150,11 @@ __global__ void __launch_bounds__(256) k_measure(const uint32_t L0, const uint32
             be += se[k];
             bm += sm[k];
         }
-        atomicAdd(&obs->e, (unsigned long long)be);
-        atomicAdd(&obs->m, (unsigned long long)bm);
-        __threadfence();
-        const unsigned int ticket = atomicAdd(&obs->done, 1u);
-        if (ticket == gridDim.x - 1) {
-            __threadfence();
-            const long long te = (long long)atomicAdd(&obs->e, 0ull);
-            const long long tm = (long long)atomicAdd(&obs->m, 0ull);
-            obs->last_e = te;
-            obs->last_m = tm;
-            if (accumulate) {
-                const double E = -(double)te / (double)n, M = (double)tm / (double)n;
-                obs->acc[0] += E;
-                obs->acc[1] += E * E;
-                obs->acc[2] += fabs(M);
-                obs->acc[3] += 1.0;
-                const unsigned long long k = obs->n_samples;
-                if (k < cap) {
-                    series[2 * k] = te;
-                    series[2 * k + 1] = tm;
-                }
-                obs->n_samples = k + 1;
-            }
-            obs->e = 0;
-            obs->m = 0;
-            obs->done = 0;
-        }
+        obs_add_part(obs, series, cap, n, gridDim.x, be, bm, accumulate);
     }
 }
 
-// LCG32_State<W>::Init for every tile (random/src/lcg32.cpp:138-160), seeds seed_base + tile.
+// LCG32_State<W>::Init for every tile (random/src/lcg32.cpp:27-49), seeds seed_base + tile.
 template <int W>
 __global__ void k_rng_init(const uint32_t n_tiles, const uint32_t seed_base, uint32_t *state, uint8_t *sel,
                            uint32_t *iter)
@@ -203,7 +181,7 @@ __global__ void k_rng_init(const uint32_t n_tiles, const uint32_t seed_base, uin
     iter[t] = 0;
 }
 
-// Hot start of Lattice<2> (ising/src/lattice.cpp:122-124): site i takes drand48 draw i + 1
+// Hot start of Lattice<2> (ising/src/lattice.cpp:24-26): site i takes drand48 draw i + 1
 // after srand48(seed); drand48() < 0.5 iff bit 47 of the 48-bit state is clear.
 __global__ void k_hot_start(const size_t n, const uint32_t seed, uint8_t *spins)
 {
@@ -261,6 +239,9 @@ struct swb_lattice {
     unsigned int *fault = nullptr;  // set by a chase that exceeded kChainCap
     int measure_grid = 0;
     uint32_t smem_flip = 0;
+    bool spins_attached = false;   // spins point at a caller-owned device buffer (swb_attach_spins)
+    bool fused_measure = false;    // the assign phase can measure the spins it starts from
+    bool measure_pending = false;  // a sample of the current spins is still to be taken
 };
 
 namespace {
@@ -272,43 +253,52 @@ int set_device(const swb_lattice *h)
     return SWB_OK;
 }
 
-template <int W, int TXc, int TYc, bool kDebug>
-int launch_assign_k(swb_lattice *h, float p_add, uint8_t *dbg_bonds, uint32_t *dbg_assign)
+template <int W, int TXc, int TYc>
+int launch_assign_k(swb_lattice *h, float p_add, const AssignDump &dump, const MeasureArgs &meas)
 {
     const Geo &g = h->g;
     // Whole warps: the draws use full-warp shuffles and ballots; surplus lanes have no tile.
     const dim3 grid(g.nbx, g.nby), block((g.TBX * g.TBY * W + 31) / 32 * 32);
-    k_assign<W, TXc, TYc, kDebug><<<grid, block, h->smem_assign, h->stream>>>(
-        g, h->spins, h->labels, h->rng_state, h->rng_sel, h->rng_iter, accept_threshold(p_add), h->edge, dbg_bonds,
-        dbg_assign);
+    if (meas.obs)
+        k_assign<W, TXc, TYc, true><<<grid, block, h->smem_assign, h->stream>>>(
+            g, h->spins, h->labels, h->rng_state, h->rng_sel, h->rng_iter, accept_threshold(p_add), h->edge, dump, meas);
+    else
+        k_assign<W, TXc, TYc, false><<<grid, block, h->smem_assign, h->stream>>>(
+            g, h->spins, h->labels, h->rng_state, h->rng_sel, h->rng_iter, accept_threshold(p_add), h->edge, dump, meas);
     SWB_LAUNCHED();
     return SWB_OK;
 }
 
+// The instance a plain sweep of this handle runs (compile-time tile shape for the common
+// shapes), with `dump` passed through; a dump of the tile-local stage takes the runtime-shape
+// instance instead, whose tile-by-tile form computes that stage.
 template <int W>
-int launch_assign_w(swb_lattice *h, float p_add, uint8_t *dbg_bonds, uint32_t *dbg_assign)
+int launch_assign_w(swb_lattice *h, float p_add, const AssignDump &dump, const MeasureArgs &meas)
 {
-    if (dbg_assign)
-        return launch_assign_k<W, 0, 0, true>(h, p_add, dbg_bonds, dbg_assign);
+    if (dump.tile_labels)
+        return launch_assign_k<W, 0, 0>(h, p_add, dump, meas);
     if constexpr (W == 16) {
         const uint32_t tx = h->g.TX, ty = h->g.TY;
-        if (tx == 16 && ty == 8) return launch_assign_k<W, 16, 8, false>(h, p_add, nullptr, nullptr);
-        if (tx == 8 && ty == 8) return launch_assign_k<W, 8, 8, false>(h, p_add, nullptr, nullptr);
-        if (tx == 32 && ty == 4) return launch_assign_k<W, 32, 4, false>(h, p_add, nullptr, nullptr);
-        if (tx == 16 && ty == 16) return launch_assign_k<W, 16, 16, false>(h, p_add, nullptr, nullptr);
-        if (tx == 8 && ty == 16) return launch_assign_k<W, 8, 16, false>(h, p_add, nullptr, nullptr);
-        if (tx == 32 && ty == 8) return launch_assign_k<W, 32, 8, false>(h, p_add, nullptr, nullptr);
-        if (tx == 16 && ty == 4) return launch_assign_k<W, 16, 4, false>(h, p_add, nullptr, nullptr);
+        if (tx == 16 && ty == 8) return launch_assign_k<W, 16, 8>(h, p_add, dump, meas);
+        if (tx == 8 && ty == 8) return launch_assign_k<W, 8, 8>(h, p_add, dump, meas);
+        if (tx == 32 && ty == 4) return launch_assign_k<W, 32, 4>(h, p_add, dump, meas);
+        if (tx == 16 && ty == 16) return launch_assign_k<W, 16, 16>(h, p_add, dump, meas);
+        if (tx == 8 && ty == 16) return launch_assign_k<W, 8, 16>(h, p_add, dump, meas);
+        if (tx == 32 && ty == 8) return launch_assign_k<W, 32, 8>(h, p_add, dump, meas);
+        if (tx == 16 && ty == 4) return launch_assign_k<W, 16, 4>(h, p_add, dump, meas);
     }
-    return launch_assign_k<W, 0, 0, false>(h, p_add, nullptr, nullptr);
+    return launch_assign_k<W, 0, 0>(h, p_add, dump, meas);
 }
 
-int launch_assign(swb_lattice *h, float p_add, uint8_t *dbg_bonds, uint32_t *dbg_assign)
+// measure: the assign phase also measures the spins it starts from (only where the block
+// labelling uses bond words: fused_measure).
+int launch_assign(swb_lattice *h, float p_add, const AssignDump &dump = AssignDump{}, bool measure = false)
 {
+    const MeasureArgs meas = measure ? MeasureArgs{h->obs, h->series, h->series_cap} : MeasureArgs{};
     switch (h->W) {
-    case 8: return launch_assign_w<8>(h, p_add, dbg_bonds, dbg_assign);
-    case 16: return launch_assign_w<16>(h, p_add, dbg_bonds, dbg_assign);
-    case 32: return launch_assign_w<32>(h, p_add, dbg_bonds, dbg_assign);
+    case 8: return launch_assign_w<8>(h, p_add, dump, meas);
+    case 16: return launch_assign_w<16>(h, p_add, dump, meas);
+    case 32: return launch_assign_w<32>(h, p_add, dump, meas);
     }
     return fail(SWB_ERR_ARGUMENT, "unsupported lcg width %u", h->W);
 }
@@ -343,9 +333,10 @@ int launch_flip(swb_lattice *h, bool write_labels)
     return SWB_OK;
 }
 
-int launch_sweep(swb_lattice *h, float p_add, bool write_labels, uint8_t *dbg_bonds, uint32_t *dbg_assign)
+int launch_sweep(swb_lattice *h, float p_add, bool write_labels, const AssignDump &dump = AssignDump{},
+                 bool measure = false)
 {
-    if (int rc = launch_assign(h, p_add, dbg_bonds, dbg_assign))
+    if (int rc = launch_assign(h, p_add, dump, measure))
         return rc;
     if (int rc = launch_merge(h))
         return rc;
@@ -358,6 +349,17 @@ int launch_measure(swb_lattice *h, int accumulate)
                                                        accumulate);
     SWB_LAUNCHED();
     return SWB_OK;
+}
+
+// A measurement of the current spins that swb_sweep left for the next sweep's assign phase to
+// make is made now, by k_measure: before anything reads the observables, changes the spins or
+// sweeps without measuring.
+int flush_measure(swb_lattice *h)
+{
+    if (!h->measure_pending)
+        return SWB_OK;
+    h->measure_pending = false;
+    return launch_measure(h, 1);
 }
 
 bool valid_width(uint32_t W) { return W == 8 || W == 16 || W == 32; }
@@ -380,6 +382,38 @@ int index_of_pair(uint32_t a, uint32_t c)
         if (lcg_param_a(s) == a && lcg_param_c(s) == c)
             return (int)s;
     return -1;
+}
+
+// One sweep with its stages dumped to host buffers (each may be null).  tile_stage: the
+// runtime-shape assign labels tile by tile and dumps the tile-local labels (the reference's
+// AssignLabels stage) into `mid`; otherwise the instance a plain sweep runs dumps the labels of
+// the bonds inside each block into `mid`.  Both dump the bonds, and the flip stores the
+// resolved labels.
+int recorded_sweep(swb_lattice *h, float temperature, bool tile_stage, uint8_t *bonds, uint32_t *mid,
+                   uint32_t *labels_final)
+{
+    AssignDump dump{};
+    if (bonds)
+        SWB_CUDA(cudaMallocAsync(&dump.bonds, h->n, h->stream));
+    if (mid || tile_stage)
+        SWB_CUDA(cudaMallocAsync(tile_stage ? &dump.tile_labels : &dump.block_labels, h->n * sizeof(uint32_t),
+                                 h->stream));
+    uint32_t *d_mid = tile_stage ? dump.tile_labels : dump.block_labels;
+    int rc = launch_sweep(h, swb_p_add(temperature), true, dump);
+    if (rc == SWB_OK) {
+        if (bonds)
+            SWB_CUDA(cudaMemcpyAsync(bonds, dump.bonds, h->n, cudaMemcpyDeviceToHost, h->stream));
+        if (mid)
+            SWB_CUDA(cudaMemcpyAsync(mid, d_mid, h->n * 4, cudaMemcpyDeviceToHost, h->stream));
+        if (labels_final)
+            SWB_CUDA(cudaMemcpyAsync(labels_final, h->labels, h->n * 4, cudaMemcpyDeviceToHost, h->stream));
+    }
+    if (dump.bonds)
+        cudaFreeAsync(dump.bonds, h->stream);
+    if (d_mid)
+        cudaFreeAsync(d_mid, h->stream);
+    SWB_CUDA(cudaStreamSynchronize(h->stream));
+    return rc ? rc : check_fault(h);
 }
 
 }  // namespace
@@ -470,6 +504,7 @@ int swb_create(swb_lattice **out, uint32_t L0, uint32_t L1, uint32_t tile_x, uin
     SWB_TRY(cudaMemsetAsync(h->spins, 0, h->n + 16, h->stream));
     SWB_TRY(cudaMemsetAsync(h->obs, 0, sizeof(Obs), h->stream));
     h->smem_flip = flip_smem_bytes(h->g);
+    h->fused_measure = (h->g.BX & 31u) == 0 && (h->g.BX & (h->g.BX - 1)) == 0;  // the bond-word labelling
     h->measure_grid = (int)std::min<size_t>((h->n + 255) / 256, (size_t)sms * 8);
     if (h->measure_grid < 1) h->measure_grid = 1;
     switch (h->W) {
@@ -492,7 +527,8 @@ int swb_destroy(swb_lattice *h)
     cudaSetDevice(h->device);
     if (h->stream)
         cudaStreamSynchronize(h->stream);
-    cudaFree(h->spins);
+    if (!h->spins_attached)
+        cudaFree(h->spins);
     cudaFree(h->labels);
     cudaFree(h->rng_state);
     cudaFree(h->rng_sel);
@@ -514,6 +550,8 @@ int swb_set_spins(swb_lattice *h, const uint8_t *host_spins)
     if (!h || !host_spins)
         return fail(SWB_ERR_ARGUMENT, "NULL argument");
     if (int rc = set_device(h))
+        return rc;
+    if (int rc = flush_measure(h))
         return rc;
     SWB_CUDA(cudaMemcpyAsync(h->spins, host_spins, h->n, cudaMemcpyHostToDevice, h->stream));
     SWB_CUDA(cudaMemsetAsync(h->scratch_flag, 0, sizeof(unsigned int), h->stream));
@@ -544,6 +582,8 @@ int swb_hot_start(swb_lattice *h, uint32_t seed)
         return fail(SWB_ERR_ARGUMENT, "NULL handle");
     if (int rc = set_device(h))
         return rc;
+    if (int rc = flush_measure(h))
+        return rc;
     const size_t chunks = (h->n + 63) / 64;
     k_hot_start<<<(unsigned)((chunks + 255) / 256), 256, 0, h->stream>>>(h->n, seed, h->spins);
     SWB_LAUNCHED();
@@ -555,6 +595,8 @@ int swb_cold_start(swb_lattice *h, uint8_t value)
     if (!h || value > 1)
         return fail(SWB_ERR_ARGUMENT, "cold start value must be 0 or 1");
     if (int rc = set_device(h))
+        return rc;
+    if (int rc = flush_measure(h))
         return rc;
     k_fill<<<h->measure_grid, 256, 0, h->stream>>>(h->n, value, h->spins);
     SWB_LAUNCHED();
@@ -571,11 +613,17 @@ int swb_sweep(swb_lattice *h, float temperature, uint32_t n_sweeps, uint32_t mea
         return rc;
     const float p_add = swb_p_add(temperature);
     for (uint32_t s = 1; s <= n_sweeps; ++s) {
-        if (int rc = launch_sweep(h, p_add, false, nullptr, nullptr))
+        // A pending sample of the spins this sweep starts from is taken by its assign phase
+        // (no extra pass over the spins), else by k_measure before the sweep.
+        const bool fused = h->measure_pending && h->fused_measure;
+        if (!fused)
+            if (int rc = flush_measure(h))
+                return rc;
+        h->measure_pending = false;
+        if (int rc = launch_sweep(h, p_add, false, AssignDump{}, fused))
             return rc;
         if (measure_every && (s % measure_every) == 0)
-            if (int rc = launch_measure(h, 1))
-                return rc;
+            h->measure_pending = true;
     }
     return SWB_OK;
 }
@@ -589,23 +637,33 @@ int swb_sweep_recorded(swb_lattice *h, float temperature, uint8_t *bonds, uint32
         return fail(SWB_ERR_ARGUMENT, "temperature must be positive and finite");
     if (int rc = set_device(h))
         return rc;
-    uint8_t *d_bonds = nullptr;
-    uint32_t *d_assign = nullptr;
-    SWB_CUDA(cudaMallocAsync(&d_bonds, h->n, h->stream));
-    SWB_CUDA(cudaMallocAsync(&d_assign, h->n * sizeof(uint32_t), h->stream));
-    int rc = launch_sweep(h, swb_p_add(temperature), true, d_bonds, d_assign);
-    if (rc == SWB_OK) {
-        if (bonds)
-            SWB_CUDA(cudaMemcpyAsync(bonds, d_bonds, h->n, cudaMemcpyDeviceToHost, h->stream));
-        if (labels_assign)
-            SWB_CUDA(cudaMemcpyAsync(labels_assign, d_assign, h->n * 4, cudaMemcpyDeviceToHost, h->stream));
-        if (labels_final)
-            SWB_CUDA(cudaMemcpyAsync(labels_final, h->labels, h->n * 4, cudaMemcpyDeviceToHost, h->stream));
-    }
-    cudaFreeAsync(d_bonds, h->stream);
-    cudaFreeAsync(d_assign, h->stream);
-    SWB_CUDA(cudaStreamSynchronize(h->stream));
-    return rc ? rc : check_fault(h);
+    if (int rc = flush_measure(h))
+        return rc;
+    return recorded_sweep(h, temperature, true, bonds, labels_assign, labels_final);
+}
+
+int swb_sweep_dumped(swb_lattice *h, float temperature, uint8_t *bonds, uint32_t *labels_block,
+                     uint32_t *labels_final)
+{
+    if (!h)
+        return fail(SWB_ERR_ARGUMENT, "NULL handle");
+    if (!(temperature > 0.0f) || !std::isfinite(temperature))
+        return fail(SWB_ERR_ARGUMENT, "temperature must be positive and finite");
+    if (int rc = set_device(h))
+        return rc;
+    if (int rc = flush_measure(h))
+        return rc;
+    return recorded_sweep(h, temperature, false, bonds, labels_block, labels_final);
+}
+
+int swb_geometry(swb_lattice *h, uint32_t *geometry)
+{
+    if (!h || !geometry)
+        return fail(SWB_ERR_ARGUMENT, "NULL argument");
+    const Geo &g = h->g;
+    const uint32_t v[8] = {g.L0, g.L1, g.TX, g.TY, g.BX, g.BY, g.nbx, g.nby};
+    std::memcpy(geometry, v, sizeof(v));
+    return SWB_OK;
 }
 
 int swb_synchronize(swb_lattice *h)
@@ -623,6 +681,8 @@ int swb_energy_magnetization(swb_lattice *h, double *out, int64_t *e_sum, int64_
     if (!h)
         return fail(SWB_ERR_ARGUMENT, "NULL handle");
     if (int rc = set_device(h))
+        return rc;
+    if (int rc = flush_measure(h))
         return rc;
     if (int rc = launch_measure(h, 0))
         return rc;
@@ -644,6 +704,8 @@ int swb_accumulators(swb_lattice *h, double *out)
         return fail(SWB_ERR_ARGUMENT, "NULL argument");
     if (int rc = set_device(h))
         return rc;
+    if (int rc = flush_measure(h))
+        return rc;
     Obs o;
     SWB_CUDA(cudaMemcpyAsync(&o, h->obs, sizeof(Obs), cudaMemcpyDeviceToHost, h->stream));
     SWB_CUDA(cudaStreamSynchronize(h->stream));
@@ -657,6 +719,7 @@ int swb_reset_accumulators(swb_lattice *h)
         return fail(SWB_ERR_ARGUMENT, "NULL handle");
     if (int rc = set_device(h))
         return rc;
+    h->measure_pending = false;  // a sample requested before the reset is dropped with the others
     SWB_CUDA(cudaMemsetAsync(h->obs, 0, sizeof(Obs), h->stream));
     return SWB_OK;
 }
@@ -666,6 +729,8 @@ int swb_samples(swb_lattice *h, int64_t *em, uint64_t capacity, uint64_t *count)
     if (!h || !count)
         return fail(SWB_ERR_ARGUMENT, "NULL argument");
     if (int rc = set_device(h))
+        return rc;
+    if (int rc = flush_measure(h))
         return rc;
     Obs o;
     SWB_CUDA(cudaMemcpyAsync(&o, h->obs, sizeof(Obs), cudaMemcpyDeviceToHost, h->stream));
@@ -735,6 +800,10 @@ int swb_device_buffers(swb_lattice *h, void **spins, void **labels)
 {
     if (!h)
         return fail(SWB_ERR_ARGUMENT, "NULL handle");
+    if (int rc = set_device(h))
+        return rc;
+    if (int rc = flush_measure(h))  // the caller may change the spins through the pointer
+        return rc;
     if (spins) *spins = h->spins;
     if (labels) *labels = h->labels;
     return SWB_OK;
@@ -756,6 +825,8 @@ int swb_sweep_timed(swb_lattice *h, float temperature, uint32_t n_sweeps, int pe
         return fail(SWB_ERR_ARGUMENT, "temperature must be positive and finite");
     if (int rc = set_device(h))
         return rc;
+    if (int rc = flush_measure(h))
+        return rc;
     const float p_add = swb_p_add(temperature);
     ms[0] = ms[1] = ms[2] = ms[3] = 0.0f;
     cudaEvent_t ev[5];
@@ -765,11 +836,11 @@ int swb_sweep_timed(swb_lattice *h, float temperature, uint32_t n_sweeps, int pe
     SWB_CUDA(cudaEventRecord(ev[0], h->stream));
     for (uint32_t s = 0; s < n_sweeps && rc == SWB_OK; ++s) {
         if (!per_kernel) {
-            rc = launch_sweep(h, p_add, false, nullptr, nullptr);
+            rc = launch_sweep(h, p_add, false);
             continue;
         }
         SWB_CUDA(cudaEventRecord(ev[1], h->stream));
-        if ((rc = launch_assign(h, p_add, nullptr, nullptr)))
+        if ((rc = launch_assign(h, p_add)))
             break;
         SWB_CUDA(cudaEventRecord(ev[2], h->stream));
         k_merge<<<dim3(h->g.nbx, h->g.nby), h->g.BX + h->g.BY, 0, h->stream>>>(h->g, h->edge, h->labels, h->fault,
@@ -802,6 +873,115 @@ int swb_sweep_timed(swb_lattice *h, float temperature, uint32_t n_sweeps, int pe
     return rc ? rc : check_fault(h);
 }
 
+int swb_attach_spins(swb_lattice *h, void *device_spins)
+{
+    if (!h || !device_spins)
+        return fail(SWB_ERR_ARGUMENT, "NULL argument");
+    if (reinterpret_cast<uintptr_t>(device_spins) % 16)
+        return fail(SWB_ERR_ARGUMENT, "device spins must be 16-byte aligned");
+    if (int rc = set_device(h))
+        return rc;
+    cudaPointerAttributes at{};
+    SWB_CUDA(cudaPointerGetAttributes(&at, device_spins));
+    if (at.type != cudaMemoryTypeDevice || at.device != h->device)
+        return fail(SWB_ERR_ARGUMENT, "spins are not device memory of CUDA device %d", h->device);
+    if (int rc = flush_measure(h))
+        return rc;
+    SWB_CUDA(cudaStreamSynchronize(h->stream));
+    if (!h->spins_attached)
+        SWB_CUDA(cudaFree(h->spins));
+    h->spins = static_cast<uint8_t *>(device_spins);
+    h->spins_attached = true;
+    return SWB_OK;
+}
+
+int swb_device_alloc(int device, size_t bytes, void **ptr)
+{
+    if (!ptr)
+        return fail(SWB_ERR_ARGUMENT, "ptr is NULL");
+    *ptr = nullptr;
+    SWB_CUDA(cudaSetDevice(device));
+    SWB_CUDA(cudaMalloc(ptr, bytes + 16));  // 256-byte aligned; 16 bytes of slack for vector accesses
+    return SWB_OK;
+}
+
+int swb_device_free(int device, void *ptr)
+{
+    if (!ptr)
+        return SWB_OK;
+    SWB_CUDA(cudaSetDevice(device));
+    SWB_CUDA(cudaFree(ptr));
+    return SWB_OK;
+}
+
+int swb_copy_to_device(int device, void *dst, const void *src, size_t bytes)
+{
+    if ((!dst || !src) && bytes)
+        return fail(SWB_ERR_ARGUMENT, "NULL argument");
+    SWB_CUDA(cudaSetDevice(device));
+    SWB_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+    return SWB_OK;
+}
+
+int swb_copy_to_host(int device, void *dst, const void *src, size_t bytes)
+{
+    if ((!dst || !src) && bytes)
+        return fail(SWB_ERR_ARGUMENT, "NULL argument");
+    SWB_CUDA(cudaSetDevice(device));
+    SWB_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
+    return SWB_OK;
+}
+
+int swb_device_synchronize(int device)
+{
+    SWB_CUDA(cudaSetDevice(device));
+    SWB_CUDA(cudaDeviceSynchronize());
+    return SWB_OK;
+}
+
+int swb_device_sm_count(int device, uint32_t *count)
+{
+    if (!count)
+        return fail(SWB_ERR_ARGUMENT, "count is NULL");
+    int v = 0;
+    SWB_CUDA(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device));
+    *count = (uint32_t)v;
+    return SWB_OK;
+}
+
+int swb_spins_energy_magnetization(int device, uint32_t L0, uint32_t L1, const void *device_spins, double *out,
+                                   int64_t *e_sum, int64_t *m_sum)
+{
+    if (!device_spins || L0 == 0 || L1 == 0)
+        return fail(SWB_ERR_ARGUMENT, "NULL spins or empty lattice");
+    // One small accumulator per device, kept until exit; calls on a device are serialised.
+    static std::mutex mu;
+    static std::vector<Obs *> acc;
+    std::lock_guard<std::mutex> lock(mu);
+    SWB_CUDA(cudaSetDevice(device));
+    if ((int)acc.size() <= device)
+        acc.resize(device + 1, nullptr);
+    if (!acc[device]) {
+        SWB_CUDA(cudaMalloc(&acc[device], sizeof(Obs)));
+        SWB_CUDA(cudaMemset(acc[device], 0, sizeof(Obs)));
+    }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const size_t n = (size_t)L0 * L1;
+    const int grid = (int)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, (size_t)sms * 8));
+    k_measure<<<grid, 256>>>(L0, L1, static_cast<const uint8_t *>(device_spins), acc[device], nullptr, 0, 0);
+    SWB_LAUNCHED();
+    Obs o;
+    SWB_CUDA(cudaMemcpy(&o, acc[device], sizeof(Obs), cudaMemcpyDeviceToHost));
+    if (out) {
+        out[0] = -(double)o.last_e / (double)n;
+        out[1] = (double)o.last_m / (double)n;
+    }
+    if (e_sum) *e_sum = o.last_e;
+    if (m_sum) *m_sum = o.last_m;
+    return SWB_OK;
+}
+
 int swb_host_alloc(void **ptr, size_t bytes)
 {
     if (!ptr)
@@ -825,8 +1005,10 @@ int swb_update_host(swb_lattice *h, float temperature, const uint8_t *spins_in, 
         return fail(SWB_ERR_ARGUMENT, "temperature must be positive and finite");
     if (int rc = set_device(h))
         return rc;
+    if (int rc = flush_measure(h))
+        return rc;
     SWB_CUDA(cudaMemcpyAsync(h->spins, spins_in, h->n, cudaMemcpyHostToDevice, h->stream));
-    if (int rc = launch_sweep(h, swb_p_add(temperature), false, nullptr, nullptr))
+    if (int rc = launch_sweep(h, swb_p_add(temperature), false))
         return rc;
     SWB_CUDA(cudaMemcpyAsync(spins_out, h->spins, h->n, cudaMemcpyDeviceToHost, h->stream));
     if (em_out) {
@@ -857,42 +1039,9 @@ int swb_update_host(swb_lattice *h, float temperature, const uint8_t *spins_in, 
 
 namespace swb {
 
-constexpr uint64_t kStaticMaxSites = 1ull << 22;               // 2048 x 2048 sites
-constexpr size_t kStaticScratchBytes = (24ull << 20) + 1024;   // labels 16 MiB + edge words + fault
-
 inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 }  // namespace swb
-
-// In host code this name is a stand-in for the array, not a device address: the address comes
-// from cudaGetSymbolAddress, once per device.
-static __device__ __align__(256) unsigned char swb_static_scratch[swb::kStaticScratchBytes];
-
-namespace {
-
-constexpr int kStaticMaxDevices = 64;
-std::mutex g_static_mutex;
-unsigned char *g_static_base[kStaticMaxDevices] = {};
-
-// Device address of swb_static_scratch on the current device (looked up on the first call).
-int static_scratch(int device, unsigned char **base)
-{
-    if (device < 0 || device >= kStaticMaxDevices)
-        return fail(SWB_ERR_ARGUMENT, "device %d out of range", device);
-    std::lock_guard<std::mutex> lock(g_static_mutex);
-    if (!g_static_base[device]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, swb_static_scratch);
-        if (e != cudaSuccess)
-            return fail(SWB_ERR_CUDA, "cudaGetSymbolAddress(swb_static_scratch) on device %d: %s", device,
-                        cudaGetErrorString(e));
-        g_static_base[device] = static_cast<unsigned char *>(p);
-    }
-    *base = g_static_base[device];
-    return SWB_OK;
-}
-
-}  // namespace
 
 extern "C" {
 
@@ -937,7 +1086,7 @@ int swb_sweep_static(void *stream, uint32_t L0, uint32_t L1, uint32_t tile_x, ui
 
     SWB_CUDA(cudaGetDevice(&h.device));
     unsigned char *base = nullptr;
-    if (int rc = static_scratch(h.device, &base))
+    if (int rc = static_scratch_base(h.device, &base))
         return rc;
     h.spins = spins;
     h.rng_state = rng_state;
@@ -952,7 +1101,7 @@ int swb_sweep_static(void *stream, uint32_t L0, uint32_t L1, uint32_t tile_x, ui
     SWB_CUDA(cudaMemsetAsync(h.fault, 0, sizeof(unsigned int), h.stream));
     const float p_add = swb_p_add(temperature);
     for (uint32_t s = 0; s < n_sweeps; ++s)
-        if (int rc = launch_sweep(&h, p_add, false, nullptr, nullptr))
+        if (int rc = launch_sweep(&h, p_add, false))
             return rc;
     if (wait) {
         unsigned int f = 0;

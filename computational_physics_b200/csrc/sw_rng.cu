@@ -1,10 +1,10 @@
 // Throughput kernel of the lcg32 generator on its own: the equivalent of the reference's
 // TestRNG --target program (random/src/test_rng.cpp, random/src/test_rng_amd_gpu.cpp:44-133,
 // random/src/test_rng_cpu.cpp).  Many independent streams, stream i seeded seed_base + i as
-// LCG32_State::Init does (random/src/lcg32.cpp:138-160); each update of a stream's W lanes
+// LCG32_State::Init does (random/src/lcg32.cpp:27-49); each update of a stream's W lanes
 // yields W numbers 2^-32 * (float)u in the order of LCG32<CPU>::NextReal (element k is lane
-// k % W after update k / W + 1, random/src/lcg32.cpp:214-240), with the parameter rotation
-// before every 15th update (random/src/lcg32.cpp:162-195).
+// k % W after update k / W + 1, random/src/lcg32.cpp:103-129), with the parameter rotation
+// before every 15th update (random/src/lcg32.cpp:51-84).
 //
 // One stream lives in the registers of a W-lane warp segment.  What a program can observe is
 // kept: the last 64 numbers of one chosen stream (the reference's 64-number buffer) and an XOR

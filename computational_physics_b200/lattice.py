@@ -19,7 +19,7 @@ def _ptr(a):
 
 
 def p_add(temperature: float) -> float:
-    """1 - exp(-2/T) in float (ising/src/swendsen_wang.cpp:207)."""
+    """1 - exp(-2/T) in float (ising/src/swendsen_wang.cpp:100)."""
     return lib().swb_p_add(temperature)
 
 
@@ -126,6 +126,23 @@ class SwendsenWang2D:
         lf = np.empty((self.L1, self.L0), np.uint32)
         check(self._lib.swb_sweep_recorded(self._h, temperature, _ptr(b), _ptr(la), _ptr(lf)))
         return b, la, lf
+
+    def update_dumped(self, temperature: float):
+        """One sweep through the kernels a plain update runs, returning (bonds, labels_block,
+        labels_final) of this sweep (labels_block: components over the bonds inside each
+        assign block, see :meth:`geometry`)."""
+        b = np.empty((self.L1, self.L0), np.uint8)
+        lb = np.empty((self.L1, self.L0), np.uint32)
+        lf = np.empty((self.L1, self.L0), np.uint32)
+        check(self._lib.swb_sweep_dumped(self._h, temperature, _ptr(b), _ptr(lb), _ptr(lf)))
+        return b, lb, lf
+
+    def geometry(self) -> dict:
+        """Tile and assign-block shape of the handle."""
+        g = np.zeros(8, np.uint32)
+        check(self._lib.swb_geometry(self._h, _ptr(g)))
+        keys = ("L0", "L1", "tile_x", "tile_y", "block_x", "block_y", "blocks_x", "blocks_y")
+        return {k: int(v) for k, v in zip(keys, g)}
 
     def update_host(self, temperature: float, spins_in: np.ndarray, spins_out: np.ndarray,
                     em: np.ndarray | None = None) -> None:

@@ -50,8 +50,8 @@ uint64_t swb_kernel_launches(void);
 
 /* Creates an L0 x L1 periodic lattice on CUDA device `device` with tiles tile_x x tile_y
  * and lcg32 streams of `lcg_width` lanes seeded seed_base + tile id.  Replaces
- * SwendsenWang_2D::Initialize (ising/src/swendsen_wang.cpp:148-199): extents must be
- * even (:154-155); at most 2^31 - 1 sites (labels are uint32, swendsen_wang.hpp:29-30, with
+ * SwendsenWang_2D::Initialize (ising/src/swendsen_wang.cpp:41-92): extents must be
+ * even (:47-48); at most 2^31 - 1 sites (labels are uint32, swendsen_wang.hpp:28-29, with
  * the top bit used internally).  tile_x in {8, 16, 32},
  * 2 <= tile_y <= 32, lcg_width in {8, 16, 32}.  Spins start all 0.  A lattice of full
  * 128 x 32-site blocks, or of at least 4096 blocks, resolves merged roots in a kernel of
@@ -66,44 +66,64 @@ int swb_create(swb_lattice **out, uint32_t L0, uint32_t L1, uint32_t tile_x, uin
 int swb_destroy(swb_lattice *h);
 
 /* Copies host spins (L0*L1 bytes, 0/1) to the device: Lattice<2>::InitializeGpuSpins
- * (ising/src/lattice.cpp:179-194).  Values other than 0/1 are rejected. */
+ * (ising/src/lattice.cpp:81-96).  Values other than 0/1 are rejected. */
 int swb_set_spins(swb_lattice *h, const uint8_t *host_spins);
 
 /* Copies the device spins to the host (L0*L1 bytes). */
 int swb_get_spins(swb_lattice *h, uint8_t *host_spins);
 
 /* Hot start on the device, bit-identical to Lattice<2>'s constructor with srand48(seed)
- * (ising/src/lattice.cpp:113-125; the reference always uses seed 1). */
+ * (ising/src/lattice.cpp:15-27; the reference always uses seed 1). */
 int swb_hot_start(swb_lattice *h, uint32_t seed);
 
 /* All spins set to `value` (0 or 1): a cold start. */
 int swb_cold_start(swb_lattice *h, uint8_t value);
 
-/* p_add = 1 - exp(-2/T) in float, as ising/src/swendsen_wang.cpp:207. */
+/* p_add = 1 - exp(-2/T) in float, as ising/src/swendsen_wang.cpp:100. */
 float swb_p_add(float temperature);
 
 /* The integer form of the bond test: a draw u is accepted iff u < swb_accept_threshold(p_add),
- * which equals the reference's (float)u * 2^-32 < p_add (random/src/lcg32.cpp:231-240). */
+ * which equals the reference's (float)u * 2^-32 < p_add (random/src/lcg32.cpp:120-129). */
 uint32_t swb_accept_threshold(float p_add);
 
-/* n_sweeps sweeps at `temperature`: SwendsenWang_2D::Update (ising/src/swendsen_wang.cpp:201-219)
+/* n_sweeps sweeps at `temperature`: SwendsenWang_2D::Update (ising/src/swendsen_wang.cpp:94-112)
  * -- bond activation + tile labelling, boundary merge, label resolution, cluster flip.  If
  * measure_every > 0, after every measure_every-th sweep the energy and magnetisation are
- * accumulated on the device (E, E^2, |M| in FP64, and the exact integer sums per sample).
+ * accumulated on the device (E, E^2, |M| in FP64, and the exact integer sums per sample).  The
+ * sample of the spins after a sweep is taken by the next sweep's assign phase, which reads those
+ * spins anyway, when the next sweep follows on this handle; otherwise (the last sweep of a
+ * call, or lattices narrower than 32 sites per block) a reduction kernel takes it before the
+ * observables are read, the spins change or an unmeasured sweep runs.  Either way the samples
+ * and their order are those of a measurement right after the sweep.
  * Asynchronous on the handle's stream; errors of the launches are reported. */
 int swb_sweep(swb_lattice *h, float temperature, uint32_t n_sweeps, uint32_t measure_every);
 
 /* Like swb_sweep with n_sweeps = 1, additionally dumping this sweep's stages to HOST buffers
  * (each may be NULL): bonds (uint8 per site), labels after tile-local labelling
- * (AssignLabels), labels after resolution (ResolveLabels).  Synchronous. */
+ * (AssignLabels), labels after resolution (ResolveLabels).  The assign phase of this sweep
+ * labels tile by tile (the reference's own stage split, ising/src/swendsen_wang.cpp:105-112),
+ * a different kernel instance from the one swb_sweep runs; swb_sweep_dumped records that one.
+ * Synchronous. */
 int swb_sweep_recorded(swb_lattice *h, float temperature, uint8_t *bonds, uint32_t *labels_assign,
                        uint32_t *labels_final);
+
+/* One sweep through the same kernels swb_sweep runs, with their dumps switched on, to HOST
+ * buffers (each may be NULL): bonds (as swb_sweep_recorded), labels_block = the minimum global
+ * site index of each site's component over the bonds inside its block (swb_geometry gives the
+ * block shape; bonds across block edges and the periodic wrap are left to the merge), and the
+ * resolved labels (ResolveLabels, ising/src/swendsen_wang_cpu.cpp:160-180).  Synchronous. */
+int swb_sweep_dumped(swb_lattice *h, float temperature, uint8_t *bonds, uint32_t *labels_block,
+                     uint32_t *labels_final);
+
+/* Geometry of the handle: geometry[0..7] = L0, L1, tile_x, tile_y, block_x, block_y (sites per
+ * assign block), blocks in x, blocks in y. */
+int swb_geometry(swb_lattice *h, uint32_t *geometry);
 
 /* Waits for all work of the handle. */
 int swb_synchronize(swb_lattice *h);
 
 /* Energy and magnetisation per site of the current spins (Lattice<2>::GetEnergyAndMagnetization,
- * ising/src/lattice.cpp:127-177), reduced on the device: out[0] = E/N, out[1] = M/N.
+ * ising/src/lattice.cpp:29-79), reduced on the device: out[0] = E/N, out[1] = M/N.
  * The exact integer sums go to e_sum / m_sum when non-NULL. */
 int swb_energy_magnetization(swb_lattice *h, double *out, int64_t *e_sum, int64_t *m_sum);
 
@@ -123,7 +143,7 @@ int swb_rng_shape(swb_lattice *h, uint32_t *n_tiles, uint32_t *lcg_width);
 
 /* Exports / imports the per-tile lcg32 streams in LCG32_State<W> terms (arrays n_tiles*W,
  * n_tiles).  Import rejects (a, c) pairs that are not one of the reference's five
- * parameter pairs (random/src/lcg32.cpp:128-135). */
+ * parameter pairs (random/src/lcg32.cpp:17-24). */
 int swb_get_rng(swb_lattice *h, uint32_t *state, uint32_t *a, uint32_t *c, uint32_t *iteration);
 int swb_set_rng(swb_lattice *h, const uint32_t *state, const uint32_t *a, const uint32_t *c,
                 const uint32_t *iteration);
@@ -145,6 +165,39 @@ int swb_sweep_timed(swb_lattice *h, float temperature, uint32_t n_sweeps, int pe
 int swb_host_alloc(void **ptr, size_t bytes);
 int swb_host_free(void *ptr);
 
+/* ---- device memory and devices, for host programs that include no CUDA header ----------- */
+
+/* Makes the handle sweep a caller-owned spin array in device memory (L0*L1 bytes, 0/1,
+ * 16-byte aligned, on the handle's device) instead of its own, which is released: the
+ * reference's Lattice<2> owns its GPU spins and hands them to the strategy
+ * (Lattice<2>::InitializeGpuSpins / RawGpuPointer, ising/include/lattice.hpp:77-80,92-94).  The
+ * buffer must outlive the handle's use of it; swb_destroy does not free it. */
+int swb_attach_spins(swb_lattice *h, void *device_spins);
+
+/* Device memory on CUDA device `device` (256-byte aligned, `bytes` plus 16 bytes of slack) and
+ * its release: the hipMalloc / GpuPointer of the reference's GPU lattice storage
+ * (ising/src/lattice.cpp:81-96, utility/hip/hip.hpp). */
+int swb_device_alloc(int device, size_t bytes, void **ptr);
+int swb_device_free(int device, void *ptr);
+
+/* Synchronous host <-> device copies (hipMemcpy in ising/src/lattice.cpp:74,89). */
+int swb_copy_to_device(int device, void *dst, const void *src, size_t bytes);
+int swb_copy_to_host(int device, void *dst, const void *src, size_t bytes);
+
+/* Waits for all work on the device: HipContext::Synchronize (utility/execution/hip_context.hpp:18-22). */
+int swb_device_synchronize(int device);
+
+/* Multiprocessor count: the default of NUM_THREADS_GPU for the GPU device
+ * (utility/device/device_amd_gpu.hpp:20). */
+int swb_device_sm_count(int device, uint32_t *count);
+
+/* Energy and magnetisation per site of any device spin array (L0 x L1, 0/1), reduced on the
+ * device: out[0] = E/N, out[1] = M/N, the integer sums to e_sum / m_sum (each may be NULL).
+ * Lattice<2>::GetEnergyAndMagnetization<AMD_GPU> copies the spins to the host for this
+ * (ising/src/lattice.cpp:70-79).  Synchronous; calls on one device are serialised. */
+int swb_spins_energy_magnetization(int device, uint32_t L0, uint32_t L1, const void *device_spins, double *out,
+                                   int64_t *e_sum, int64_t *m_sum);
+
 /* One sweep through HOST spin buffers, as the reference's Lattice<2> keeps them: copy
  * spins_in to the device, sweep, read the spins back to spins_out and the energy and
  * magnetisation per site to em_out[2] (may be NULL).  Synchronous. */
@@ -156,7 +209,7 @@ int swb_update_host(swb_lattice *h, float temperature, const uint8_t *spins_in, 
  * (an FFI caller's own lattice storage, a pool holding the whole HBM budget), where a per-call
  * cudaMalloc can fail and a cudaFree would synchronise the device.  Device buffers, on the
  * current device: spins[L0*L1] (0/1, 16-byte aligned), rng_state[n_tiles*W], rng_sel[n_tiles*W]
- * (index 0..4 of the lcg32 parameter pair, random/src/lcg32.cpp:128-135), rng_iter[n_tiles],
+ * (index 0..4 of the lcg32 parameter pair, random/src/lcg32.cpp:17-24), rng_iter[n_tiles],
  * n_tiles = ceil(L0/tile_x) * ceil(L1/tile_y) -- the layout swb_get_rng exports.  Results equal
  * swb_sweep's on the same state.  The label array, block edge words and fault word live in one
  * static device array of 24 MiB + 1 KiB, so L0*L1 is at most 4,194,304 (2048 x 2048); larger
@@ -164,8 +217,13 @@ int swb_update_host(swb_lattice *h, float temperature, const uint8_t *spins_in, 
  * (each call clears its fault word, the kernels overwrite the rest): calls that overlap on the
  * GPU race, so serialise them (one stream, or events).  The first call on each device looks the
  * array's address up (cudaGetSymbolAddress, with that device current); make that first call
- * before any stream capture.  Asynchronous on `stream` (NULL = default stream); with wait != 0
- * the call synchronises the stream and reports a label-chase fault as SWB_ERR_STATE. */
+ * before any stream capture.  The array is reserved on a device (and held until the process
+ * exits) only once this entry point has been called there.  The merged block roots are always
+ * resolved by the flip itself (the three-kernel form of swb_sweep; at 2048 x 2048 about 5 %
+ * slower than the four-kernel form swb_sweep uses there): the array has no room for the merge
+ * slots.  Asynchronous on `stream` (NULL = default stream); with wait != 0 the call
+ * synchronises the stream and reports a label-chase fault as SWB_ERR_STATE.  With wait == 0 such
+ * a fault is not reported: the next call clears the fault word. */
 int swb_sweep_static(void *stream, uint32_t L0, uint32_t L1, uint32_t tile_x, uint32_t tile_y, uint32_t lcg_width,
                      float temperature, uint32_t n_sweeps, uint8_t *spins, uint32_t *rng_state, uint8_t *rng_sel,
                      uint32_t *rng_iter, int wait);
@@ -176,7 +234,7 @@ int swb_sweep_static(void *stream, uint32_t L0, uint32_t L1, uint32_t tile_x, ui
  * (random/src/test_rng.cpp, random/src/test_rng_amd_gpu.cpp:44-133): n_streams streams of
  * lcg_width lanes, stream i seeded seed_base + i (LCG32_State::Init), each advanced
  * updates_per_stream times (a positive multiple of 64 / lcg_width); every update yields
- * lcg_width numbers 2^-32 * (float)u in NextReal order (random/src/lcg32.cpp:214-240).
+ * lcg_width numbers 2^-32 * (float)u in NextReal order (random/src/lcg32.cpp:103-129).
  * report[64] receives the last 64 numbers of stream report_id (the reference's 64-number
  * buffer), *checksum the XOR of the bit patterns of every number generated, *ms the kernel
  * time (CUDA events, stream initialisation included).  Synchronous. */

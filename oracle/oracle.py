@@ -84,6 +84,7 @@ class Oracle:
         lib.orc_sw_sweep.argtypes = [_U, _U, _U, _U, _U, _F, _P, _P, _P, _P, _P, _P, _P, _P]
         lib.orc_sw_sweep.restype = ctypes.c_int
         lib.orc_energy_magnetization.argtypes = [_U, _U, _P, _P, _P]
+        lib.orc_block_labels.argtypes = [_U, _U, _U, _U, _P, _P]
         self.lib = lib
 
     def hot_start(self, L0: int, L1: int, seed: int = 1) -> np.ndarray:
@@ -127,6 +128,15 @@ class Oracle:
         if rc != 0:
             raise ValueError(f"orc_sw_sweep failed with status {rc}")
         return (bonds, la, lf) if dumps else None
+
+    def block_labels(self, bonds: np.ndarray, block_x: int, block_y: int) -> np.ndarray:
+        """Minimum-index labels of the components over the bonds inside each block_x x
+        block_y block (the GPU path's labels between its assign and merge phases)."""
+        L1, L0 = bonds.shape
+        b = np.ascontiguousarray(bonds, np.uint8)
+        out = np.empty((L1, L0), np.uint32)
+        self.lib.orc_block_labels(L0, L1, block_x, block_y, _ptr(b), _ptr(out))
+        return out
 
     def energy_magnetization(self, spins: np.ndarray) -> tuple[int, int]:
         L1, L0 = spins.shape

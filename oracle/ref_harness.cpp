@@ -8,7 +8,7 @@
 //
 // What it adds on top of the reference:
 //   * one lcg32 stream per tile, seeded seed_base + tile_id (the reference seeds
-//     its per-thread streams i + 1, ising/src/swendsen_wang.cpp:173-180; running
+//     its per-thread streams i + 1, ising/src/swendsen_wang.cpp:66-73; running
 //     the CPU path with NUM_THREADS = number of tiles gives exactly this), by
 //     driving AssignLabels / MergeLabels with a ThreadContext whose thread id is
 //     the tile id (ising/src/swendsen_wang_cpu.cpp:16-31, 53-66);
@@ -189,17 +189,17 @@ extern "C"
     // Lane count W of the reference's lcg32 in this build (the host's SIMD width for uint32).
     int ref_lcg32_width() { return static_cast<int>(CPU::WavefrontSize<std::uint32_t>()); }
 
-    // p_add exactly as ising/src/swendsen_wang.cpp:207.
+    // p_add exactly as ising/src/swendsen_wang.cpp:100.
     float ref_p_add(float temperature) { return 1.0f - static_cast<float>(std::exp(-2.0f / temperature)); }
 
-    // Hot start of Lattice<2> (ising/src/lattice.cpp:113-125): srand48(1), drand48() < 0.5 ? 0 : 1.
+    // Hot start of Lattice<2> (ising/src/lattice.cpp:15-27): srand48(1), drand48() < 0.5 ? 0 : 1.
     void ref_hot_start(std::uint32_t L0, std::uint32_t L1, std::uint8_t* spins)
     {
         Lattice<2> lattice({L0, L1});
         std::memcpy(spins, lattice.RawPointer(), lattice.NumSites());
     }
 
-    // LCG32_State<W>::Init (random/src/lcg32.cpp:138-160).
+    // LCG32_State<W>::Init (random/src/lcg32.cpp:27-49).
     void ref_lcg32_init(std::uint32_t seed, std::uint32_t* state, std::uint32_t* a, std::uint32_t* c, std::uint32_t* iteration)
     {
         struct S : LCG32<DeviceName::CPU>::State
@@ -217,7 +217,7 @@ extern "C"
     }
 
     // LCG32<CPU>::NextReal(vector) called repeatedly with chunk sizes sizes[0..k-1]
-    // on a stream seeded `seed` (random/src/lcg32.cpp:197-240).  Writes the raw
+    // on a stream seeded `seed` (random/src/lcg32.cpp:86-129).  Writes the raw
     // float bit patterns back to back.
     void ref_lcg32_next_real(std::uint32_t seed, const std::uint32_t* sizes, std::uint32_t k, float* out)
     {
@@ -232,7 +232,7 @@ extern "C"
         }
     }
 
-    // Energy and magnetization per site (ising/src/lattice.cpp:127-165).
+    // Energy and magnetization per site (ising/src/lattice.cpp:29-67).
     void ref_energy_magnetization(std::uint32_t L0, std::uint32_t L1, const std::uint8_t* spins, double* e, double* m)
     {
         Lattice<2> lattice({L0, L1});
@@ -270,7 +270,7 @@ extern "C"
     }
 
     // The reference's own multi-threaded path: SwendsenWang_2D<LCG32, CPU>::Update
-    // (ising/src/swendsen_wang.cpp:201-219) on `count` independent lattices, using a
+    // (ising/src/swendsen_wang.cpp:94-112) on `count` independent lattices, using a
     // CPU device with `num_threads` threads (the NUM_THREADS of the reference).
     // Each lattice gets its own strategy object, so lattices of different sizes can
     // be swept in one process.  Returns the wall seconds spent in the sweeps.

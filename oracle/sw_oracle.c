@@ -19,7 +19,7 @@ double orc_drand48(uint64_t *x)
     return ldexp((double)*x, -48);
 }
 
-/* ising/src/lattice.cpp:122-124 */
+/* ising/src/lattice.cpp:24-26 */
 void orc_hot_start(uint32_t L0, uint32_t L1, uint32_t seed, uint8_t *spins)
 {
     uint64_t x;
@@ -29,7 +29,7 @@ void orc_hot_start(uint32_t L0, uint32_t L1, uint32_t seed, uint8_t *spins)
         spins[i] = orc_drand48(&x) < 0.5 ? 0 : 1;
 }
 
-/* Numerical Recipes LCG parameter pairs (a, c) chosen per lane (random/src/lcg32.cpp:128-135). */
+/* Numerical Recipes LCG parameter pairs (a, c) chosen per lane (random/src/lcg32.cpp:17-24). */
 static const uint32_t kParams[5][2] = {
     {1372383749u, 1289706101u},
     {2891336453u, 1640531513u},
@@ -43,7 +43,7 @@ static int valid_width(uint32_t W)
     return W >= 2 && W <= 64 && (W & (W - 1)) == 0;
 }
 
-/* random/src/lcg32.cpp:138-160 */
+/* random/src/lcg32.cpp:27-49 */
 void orc_lcg32_init(uint32_t W, uint32_t seed, uint32_t *state, uint32_t *a, uint32_t *c, uint32_t *iteration)
 {
     uint64_t x;
@@ -59,7 +59,7 @@ void orc_lcg32_init(uint32_t W, uint32_t seed, uint32_t *state, uint32_t *a, uin
     *iteration = 0;
 }
 
-/* random/src/lcg32.cpp:162-195: every 15th update first rotates the (a, c) pairs by
+/* random/src/lcg32.cpp:51-84: every 15th update first rotates the (a, c) pairs by
  * state[iteration & (W-1)] + (iteration odd ? 0 : 1), then every lane steps. */
 void orc_lcg32_update(uint32_t W, uint32_t *state, uint32_t *a, uint32_t *c, uint32_t *iteration)
 {
@@ -77,7 +77,7 @@ void orc_lcg32_update(uint32_t W, uint32_t *state, uint32_t *a, uint32_t *c, uin
         state[i] = a[i] * state[i] + c[i];
 }
 
-/* random/src/lcg32.cpp:214-240: element k of a request for n numbers is lane k % W after
+/* random/src/lcg32.cpp:103-129: element k of a request for n numbers is lane k % W after
  * update k / W + 1 of this request (the tail shorter than W also takes a fresh update);
  * the float is (float)u * 2^-32 with u rounded to nearest. */
 void orc_lcg32_next_real(uint32_t W, uint32_t *state, uint32_t *a, uint32_t *c, uint32_t *iteration,
@@ -90,7 +90,7 @@ void orc_lcg32_next_real(uint32_t W, uint32_t *state, uint32_t *a, uint32_t *c, 
     }
 }
 
-/* ising/src/swendsen_wang.cpp:207 */
+/* ising/src/swendsen_wang.cpp:100 */
 float orc_p_add(float temperature)
 {
     return 1.0f - (float)expf(-2.0f / temperature);
@@ -134,7 +134,7 @@ int orc_sw_sweep(uint32_t L0, uint32_t L1, uint32_t tx, uint32_t ty, uint32_t W,
                  uint8_t *spins, uint32_t *rng_state, uint32_t *rng_a, uint32_t *rng_c, uint32_t *rng_iteration,
                  uint8_t *bonds, uint32_t *labels_assign, uint32_t *labels_final)
 {
-    if (L0 % 2 || L1 % 2) /* ising/src/swendsen_wang.cpp:154-155 */
+    if (L0 % 2 || L1 % 2) /* ising/src/swendsen_wang.cpp:47-48 */
         return 1;
     if (!valid_width(W))
         return 2;
@@ -234,7 +234,7 @@ int orc_sw_sweep(uint32_t L0, uint32_t L1, uint32_t tx, uint32_t ty, uint32_t W,
     return 0;
 }
 
-/* ising/src/lattice.cpp:146-164 */
+/* ising/src/lattice.cpp:48-66 */
 void orc_energy_magnetization(uint32_t L0, uint32_t L1, const uint8_t *spins, int64_t *e, int64_t *m)
 {
     int64_t ee = 0, mm = 0;
@@ -248,4 +248,22 @@ void orc_energy_magnetization(uint32_t L0, uint32_t L1, const uint8_t *spins, in
     }
     *e = ee;
     *m = mm;
+}
+
+void orc_block_labels(uint32_t L0, uint32_t L1, uint32_t BX, uint32_t BY, const uint8_t *bonds, uint32_t *out)
+{
+    const size_t n = (size_t)L0 * L1;
+    for (size_t s = 0; s < n; ++s)
+        out[s] = (uint32_t)s;
+    for (uint32_t y = 0; y < L1; ++y) {
+        for (uint32_t x = 0; x < L0; ++x) {
+            size_t s = (size_t)y * L0 + x;
+            if ((bonds[s] & 1) && x + 1 < L0 && (x + 1) % BX != 0)
+                uf_union(out, (uint32_t)s, (uint32_t)(s + 1));
+            if ((bonds[s] & 2) && y + 1 < L1 && (y + 1) % BY != 0)
+                uf_union(out, (uint32_t)s, (uint32_t)(s + L0));
+        }
+    }
+    for (size_t s = 0; s < n; ++s)
+        out[s] = uf_find(out, (uint32_t)s);
 }

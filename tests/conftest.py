@@ -32,6 +32,13 @@ def golden8():
 
 
 @pytest.fixture(scope="session")
+def c3_fixtures():
+    import json
+    with open(os.path.join(ROOT, "tests", "golden", "c3_sha.json")) as f:
+        return json.load(f)
+
+
+@pytest.fixture(scope="session")
 def gpu():
     """The native library with at least one CUDA device; GPU tests fail loudly without them."""
     import computational_physics_b200 as cp

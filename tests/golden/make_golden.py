@@ -1,6 +1,6 @@
 """Generates the golden fixtures in this directory from the UNMODIFIED reference.
 
-Needs the reference sources (default /root/reference) and the harness built by
+Needs the reference sources (--ref, else $SWB_REFERENCE_DIR, else /root/reference) and the harness built by
 ``make -C oracle ref``.  Run from the repository root:
 
     python tests/golden/make_golden.py [--ref /root/reference]
@@ -106,9 +106,15 @@ def make(width: int) -> None:
     np.savez_compressed(os.path.join(OUT, f"golden_w{width}.npz"), **d)
 
 
+# (L, num_sweeps, tile_x): small runs, one whose sweep count is not a multiple of the 10-sweep
+# measurement block (the loop runs ceil(n/10) blocks and divides by n/10), and the CPU config's
+# full protocol (128 x 128, 1000 warm-up + 100000 sweeps, 128 tiles of 16 x 8).
+CLI_RUNS = [(32, 200, 16), (64, 100, 16), (32, 205, 16), (128, 100000, 16)]
+
+
 def make_cli() -> None:
     runs = []
-    for (L, sweeps, tile_x) in [(32, 200, 16), (64, 100, 16)]:
+    for (L, sweeps, tile_x) in CLI_RUNS:
         nt = num_tiles(L, L, tile_x, 8)
         env = dict(os.environ, NUM_THREADS=str(nt))
         exe = os.path.join(ROOT, "oracle", "_ref", "Ising2D_w16")
@@ -138,13 +144,19 @@ def make_exact() -> None:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("SWB_REFERENCE_DIR", "/root/reference"))
+    ap.add_argument("--only", default="", help="comma-separated subset of w16,w8,cli,exact")
     args = ap.parse_args()
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={args.ref}"], check=True)
-    make(16)
-    make(8)
-    make_cli()
-    make_exact()
+    only = set(args.only.split(",")) if args.only else {"w16", "w8", "cli", "exact"}
+    if "w16" in only:
+        make(16)
+    if "w8" in only:
+        make(8)
+    if "cli" in only:
+        make_cli()
+    if "exact" in only:
+        make_exact()
 
 
 if __name__ == "__main__":

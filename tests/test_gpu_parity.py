@@ -2,7 +2,8 @@
 
 Small cases compare against the committed dumps of the unmodified reference
 (tests/golden/); larger ones against the C restatement (oracle/), which those dumps pin;
-the largest ones through size-independent invariants."""
+the largest ones (4096^2 - 16384^2) against digests of the restatement's output
+(tests/golden/c3_sha.json)."""
 import hashlib
 
 import numpy as np
@@ -108,6 +109,56 @@ def test_sweeps_bit_exact_vs_oracle(gpu, oracle, L0, L1, tile, W, T, sweeps):
         assert sw.energy_magnetization_sums() == (e, m)
 
 
+@pytest.mark.parametrize("L0,L1,tile,W,T,sweeps", CASES)
+def test_production_sweep_bit_exact_vs_oracle(gpu, oracle, L0, L1, tile, W, T, sweeps):
+    """The kernels a plain sweep runs, with their dumps on: bonds, the labels over the bonds
+    inside each assign block, resolved labels, flipped spins and lcg32 streams."""
+    spins = oracle.hot_start(L0, L1, 1)
+    rng = oracle.rng_init(W, num_tiles(L0, L1, *tile), 1)
+    with gpu.SwendsenWang2D(L0, L1, tile, W, 1) as sw:
+        geo = sw.geometry()
+        sw.set_spins(spins)
+        for s in range(sweeps - 1):
+            oracle.sweep(spins, tile[0], tile[1], rng, T=T)
+        sw.update(T, sweeps - 1)
+        bonds, _, lf = oracle.sweep(spins, tile[0], tile[1], rng, T=T, dumps=True)
+        gb, glb, glf = sw.update_dumped(T)
+        assert np.array_equal(gb, bonds)
+        assert np.array_equal(glb, oracle.block_labels(bonds, geo["block_x"], geo["block_y"]))
+        assert np.array_equal(glf, lf)
+        assert np.array_equal(sw.get_spins(), spins)
+        st, a, c, it = sw.get_rng()
+        assert np.array_equal(st, rng.state) and np.array_equal(it, rng.iteration)
+        assert np.array_equal(a, rng.a) and np.array_equal(c, rng.c)
+
+
+@pytest.mark.parametrize("L", [4096, 8192, 16384])
+def test_bandwidth_sizes_bit_exact(gpu, c3_fixtures, L):
+    """4096^2 - 16384^2 (tile 16 x 8, W = 16, hot start, T_c): the third sweep of the kernels a
+    plain sweep runs, digest for digest against the CPU restatement (tests/golden/c3_sha.json;
+    the 4096^2 digests also agree with the unmodified reference sources)."""
+    fx = c3_fixtures
+    want = fx["cases"][str(L)]
+    T = fx["temperature"]
+    with gpu.SwendsenWang2D(L, L, tuple(fx["tile"]), fx["lcg_width"], fx["seed_base"]) as sw:
+        geo = sw.geometry()
+        sw.hot_start(fx["hot_start_seed"])
+        sw.update(T, fx["sweeps_before"])
+        assert sha(sw.get_spins()).hex() == want["spins_in"]
+        bonds, lb, lf = sw.update_dumped(T)
+        assert sha(bonds).hex() == want["bonds"]
+        del bonds
+        if [geo["block_x"], geo["block_y"]] == fx["block"]:
+            assert sha(lb).hex() == want["labels_block"]
+        del lb
+        assert sha(lf).hex() == want["labels_final"]
+        del lf
+        assert sha(sw.get_spins()).hex() == want["spins_out"]
+        st, _, _, it = sw.get_rng()
+        assert sha(st).hex() == want["rng_state"]
+        assert sha(it).hex() == want["rng_iteration"]
+
+
 @pytest.mark.parametrize("resolve_min", ["1", "1000000000"])
 @pytest.mark.parametrize("L0,L1,tile,W,T,sweeps", [CASES[0], CASES[3], CASES[4], CASES[7]])
 def test_resolve_kernel_and_chasing_flip_agree_with_oracle(gpu, oracle, monkeypatch, resolve_min, L0, L1, tile, W, T,
@@ -116,6 +167,7 @@ def test_resolve_kernel_and_chasing_flip_agree_with_oracle(gpu, oracle, monkeypa
     (threshold above any lattice): both bit-exact with the oracle, stage dumps included."""
     monkeypatch.setenv("SWB_RESOLVE_MIN_BLOCKS", resolve_min)
     test_sweeps_bit_exact_vs_oracle(gpu, oracle, L0, L1, tile, W, T, sweeps)
+    test_production_sweep_bit_exact_vs_oracle(gpu, oracle, L0, L1, tile, W, T, sweeps)
 
 
 def test_set_rng_roundtrip_and_continue(gpu, oracle):
@@ -131,39 +183,6 @@ def test_set_rng_roundtrip_and_continue(gpu, oracle):
         for _ in range(5):
             oracle.sweep(spins, 16, 8, rng, T=2.2691853)
         assert np.array_equal(sw.get_spins(), spins)
-
-
-def test_invariants_at_16384(gpu):
-    """Size-independent properties at the bandwidth config's largest lattice: labels are
-    roots and minimal (label <= site index, label[label] == label), every bond joins equal
-    spins, flipping follows the label parity, and a resweep is deterministic."""
-    L = 16384
-    with gpu.SwendsenWang2D(L, L, (16, 8), 16) as sw:
-        sw.hot_start(1)
-        sw.update(2.2691853, 2)
-        before = sw.get_spins()
-        bonds, la, lf = sw.update_recorded(2.2691853)
-        after = sw.get_spins()
-    flat = lf.ravel()
-    R = 512
-    for y0 in range(0, L, R):
-        rows = slice(y0, y0 + R)
-        idx = np.arange(y0 * L, (y0 + R) * L, dtype=np.uint32).reshape(R, L)
-        f = lf[rows]
-        assert np.all(f <= idx)
-        assert np.array_equal(flat[f.ravel()], f.ravel())
-        assert np.all(la[rows] >= f)
-        down = np.concatenate([lf[y0 + 1:y0 + R], lf[(y0 + R) % L][None]])
-        sdown = np.concatenate([before[y0 + 1:y0 + R], before[(y0 + R) % L][None]])
-        b = bonds[rows]
-        s = before[rows]
-        xb = (b & 1).astype(bool)
-        yb = (b & 2).astype(bool)
-        assert np.all(s[xb] == np.roll(s, -1, axis=1)[xb])
-        assert np.all(s[yb] == sdown[yb])
-        assert np.all(f[xb] == np.roll(f, -1, axis=1)[xb])
-        assert np.all(f[yb] == down[yb])
-        assert np.array_equal(after[rows], s ^ (f & 1).astype(np.uint8))
 
 
 def test_errors_are_reported(gpu):
@@ -199,6 +218,34 @@ def test_measurement_accumulators(gpu, oracle):
     assert acc[0] == pytest.approx(sum(E), abs=1e-12)
     assert acc[1] == pytest.approx(sum(x * x for x in E), abs=1e-12)
     assert acc[2] == pytest.approx(sum(M), abs=1e-12)
+
+
+@pytest.mark.parametrize("L0,L1,tile", [(256, 128, (16, 8)), (8, 64, (8, 8)), (200, 96, (8, 8))])
+def test_measurement_taken_by_the_next_sweep(gpu, oracle, L0, L1, tile):
+    """Samples every 10 sweeps: the sample of the spins after sweep k is taken by sweep k + 1's
+    assign phase (no k_measure launch while sweeps follow), the last one when the observables are
+    read; all exact.  The 8-wide lattice's blocks are narrower than a 32-site word, so there
+    every sample is taken by k_measure."""
+    spins = oracle.hot_start(L0, L1, 1)
+    rng = oracle.rng_init(16, num_tiles(L0, L1, *tile), 1)
+    with gpu.SwendsenWang2D(L0, L1, tile, 16) as sw:
+        sw.set_spins(spins)
+        fused = sw.geometry()["block_x"] % 32 == 0
+        n0 = gpu.kernel_launches()
+        sw.update(2.2691853, 40, measure_every=10)
+        launched = gpu.kernel_launches() - n0
+        samples = sw.samples()
+        acc = sw.accumulators()
+        per_sweep = sw.launches_per_sweep()
+    assert launched == 40 * per_sweep + (0 if fused else 3)
+    want = []
+    for k in range(40):
+        oracle.sweep(spins, tile[0], tile[1], rng, T=2.2691853)
+        if (k + 1) % 10 == 0:
+            want.append(oracle.energy_magnetization(spins))
+    assert [tuple(x) for x in samples] == want
+    E = [-e / (L0 * L1) for e, _ in want]
+    assert acc[3] == 4 and acc[0] == pytest.approx(sum(E), abs=1e-12)
 
 
 def test_update_host_matches_device_path(gpu, oracle):

@@ -112,22 +112,28 @@ def test_restatement_reproduces_reference_cli(oracle):
     runs = json.load(open(os.path.join(GOLDEN, "ising2d_cli.json")))
     for run in runs:
         L, sweeps = run["L"], run["num_sweeps"]
+        if L * L * sweeps > 64 * 64 * 1000:
+            continue  # the 128 x 128 x 100000 protocol is pinned on the GPU (tests/test_gpu_cli.py)
         tx, ty = run["tile"]
         T = np.float32(2.2691853142130221)
         spins = oracle.hot_start(L, L, 1)
         rng = oracle.rng_init(16, num_tiles(L, L, tx, ty), 1)
         for _ in range(1000):
             oracle.sweep(spins, tx, ty, rng, T=float(T))
-        E, M = [], []
-        for _ in range(sweeps // 10):
+        # ising/src/ising_2d.cpp:127-162: blocks of 10 sweeps while i < n_sweeps, a sample after
+        # each, summed in order in double; the averages divide by n_sweeps / 10 (integer)
+        energy = energy2 = mag = 0.0
+        for _ in range(0, sweeps, 10):
             for _ in range(10):
                 oracle.sweep(spins, tx, ty, rng, T=float(T))
             e, m = oracle.energy_magnetization(spins)
-            E.append(-e / (L * L))
-            M.append(abs(m / (L * L)))
-        E = np.array(E)
-        heat = (np.mean(E * E) - E.mean() ** 2) * L * L / (T * T)
+            e, m = -1.0 * e / (L * L), 1.0 * m / (L * L)
+            energy += e
+            energy2 += e * e
+            mag += abs(m)
+        samples = sweeps // 10
+        heat = (energy2 / samples - (energy / samples) * (energy / samples)) * (L * L) / float(T * T)
         printed = run["printed"]
-        assert f"{E.mean():g}" == printed["Internal energy per spin"]
+        assert f"{energy / samples:g}" == printed["Internal energy per spin"]
         assert f"{heat:g}" == printed["Heat capacity per spin"]
-        assert f"{np.mean(M):g}" == printed["Absolute Magnetization per spin"]
+        assert f"{mag / samples:g}" == printed["Absolute Magnetization per spin"]

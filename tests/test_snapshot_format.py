@@ -43,3 +43,20 @@ def test_load_rejects_spins_of_another_extent(tmp_path):
                          "spins": np.zeros((32, 32), np.uint8)})
     with pytest.raises(ValueError, match="extent"):
         snapshot.load(path)
+
+
+def test_path_without_suffix_round_trips(tmp_path):
+    """save('job1') and load('job1') name the same file (numpy appends .npz on save)."""
+    path = str(tmp_path / "job1")
+    snapshot.save(path, {"L0": 32, "L1": 16, "tile": (16, 8), "lcg_width": 16,
+                         "spins": np.zeros((16, 32), np.uint8)})
+    assert snapshot.load(path)["L0"] == 32
+
+
+def test_load_rejects_streams_of_another_width(tmp_path):
+    path = str(tmp_path / "w.npz")
+    z = np.zeros((8, 8), np.uint32)  # 32 x 16 with 16 x 8 tiles has 4 tiles; W = 16 wanted
+    snapshot.save(path, {"L0": 32, "L1": 16, "tile": (16, 8), "lcg_width": 16, "spins": np.zeros((16, 32), np.uint8),
+                         "rng_state": z, "rng_a": z, "rng_c": z, "rng_iteration": np.zeros(4, np.uint32)})
+    with pytest.raises(ValueError, match="rng_state"):
+        snapshot.load(path)

@@ -10,7 +10,7 @@ from computational_physics_b200._native import lib
 
 T_C = 2.2691853
 PAIRS = [(1372383749, 1289706101), (2891336453, 1640531513), (2024337845, 797082193),
-         (32310901, 626627237), (29943829, 1013904223)]   # random/src/lcg32.cpp:128-135
+         (32310901, 626627237), (29943829, 1013904223)]   # random/src/lcg32.cpp:17-24
 
 
 def _sel(a, c):
