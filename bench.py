@@ -9,15 +9,21 @@ A step is one Swendsen-Wang sweep over the whole workload.  Workloads (synthetic
                T uniform in [2.0, 2.6], hot start per lattice seed, one batched sweep per
                step (the headline workload, about 40 M sites)
   plain16384   one 16384^2 lattice at T_c, tile 16x8, lcg32 W = 16, hot start
+  plain8192, plain4096   the same at 8192^2 and 4096^2
   plain1024    one 1024^2 lattice at T_c, tile 8x8, lcg32 W = 16, hot start
+  serving      Poisson job streams at 10 / 100 / 1000 jobs per second
 
 `value` is spin-updates/s of the whole job with the spins resident in HBM; `e2e` is the same
 metric through the C ABI with HOST spin buffers (copies in the timed region).  The reference
 arm (--impl reference) times the reference's own CPU path (built from its sources under
 oracle/_ref) on this host's cores, on the same workload.
 
-Multi-GPU: one process per GPU (torchrun); every rank sweeps its own copy of the workload
-(weak scaling, no collective on the data path); the time is the max over ranks.
+Multi-GPU: one process per GPU (torchrun), no collective on the data path; the time is the
+max over ranks.  The batched mix is sharded: every lattice lives on one rank (partition by
+device bytes, computational_physics_b200/shard.py), each rank sweeps its share, the value counts
+the whole mix (strong scaling), and the per-lattice observables are gathered on rank 0.  Serving
+shards the job stream the same way.  A single lattice does not shard (cross-GPU labelling would
+need iterative label exchange): plain workloads run one replica per rank (weak scaling).
 """
 from __future__ import annotations
 
@@ -103,6 +109,14 @@ class Dist:
         t = torch.tensor([x], dtype=torch.float64, device=self.device)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
+
+    def gather_object(self, obj):
+        """Every rank's `obj` as a list on rank 0 (None on the other ranks); host data only."""
+        if not self.pg:
+            return [obj]
+        out = [None] * self.world if self.rank == 0 else None
+        self.pg.gather_object(obj, out, dst=0)
+        return out
 
     def close(self):
         if self.pg:
@@ -442,11 +456,34 @@ def bench_plain(args, dist: Dist, cp) -> dict:
     }
 
 
-def build_mix(cp, device: int, lcg_width: int = 16):
+def mix_shards(world: int, lcg_width: int = 16):
+    """The mix's lattice indices per rank, balanced by the batched engine's device bytes."""
+    from computational_physics_b200 import autotune, shard
+    table = autotune.load(lcg_width=lcg_width)
+    weights = [shard.lattice_bytes(L, L, autotune.choice(L, table)[0], lcg_width) for L, _, _ in mix_workload()]
+    parts = shard.partition(weights, world)
+    return parts, shard.imbalance(parts, weights)
+
+
+def mix_observables(b, ids, index) -> dict:
+    """{mix index: [e, m]} of the lattices' current spins (integer sums over sites of
+    s (s_right + s_down) and s), read back to the host."""
+    out = {}
+    for lid, k in zip(ids, index):
+        s = b.get_spins(lid).astype(np.int64) * 2 - 1
+        e = int(np.sum(s * (np.roll(s, -1, axis=1) + np.roll(s, -1, axis=0))))
+        out[k] = [e, int(s.sum())]
+    return out
+
+
+def build_mix(cp, device: int, lcg_width: int = 16, subset=None):
+    """The batched engine holding the mix's lattices (all, or the indices in `subset`)."""
     from computational_physics_b200 import autotune
     table = autotune.load(lcg_width=lcg_width)
     mix = mix_workload()
-    b = cp.BatchedSW(capacity=len(mix), lcg_width=lcg_width, device=device)
+    if subset is not None:
+        mix = [mix[k] for k in subset]
+    b = cp.BatchedSW(capacity=max(1, len(mix)), lcg_width=lcg_width, device=device)
     ids, tiles = [], []
     for L, T, seed in mix:
         tile, block = autotune.choice(L, table)
@@ -511,9 +548,15 @@ def energy_gate(cp, device: int, warmup: int = 1000, sweeps: int = 10000, every:
 
 
 def bench_batched(args, dist: Dist, cp) -> dict:
+    """The 512-lattice mix, sharded: each lattice lives on one rank (partition by device bytes),
+    every rank sweeps its share, and the value counts the whole mix over the slowest rank."""
+    from computational_physics_b200 import shard
     dev = dist.local_rank
-    b, mix, ids, tiles, table = build_mix(cp, dev)
-    sites = sum(L * L for L, _, _ in mix)
+    parts, imbalance = mix_shards(dist.world)
+    mine = parts[dist.rank]
+    b, mix, ids, tiles, table = build_mix(cp, dev, subset=mine)
+    sites = sum(L * L for L, _, _ in mix)                      # this rank's share
+    sites_all = sum(L * L for L, _, _ in mix_workload())       # the whole mix
     b.sweep(args.warmup)
     b.synchronize()
     launches0 = cp.kernel_launches()
@@ -523,7 +566,7 @@ def bench_batched(args, dist: Dist, cp) -> dict:
     launches = cp.kernel_launches() - launches0
     dist.barrier()
     ms_max = dist.max(ms)
-    value = dist.world * sites * args.steps / (ms_max / 1e3)
+    value = sites_all * args.steps / (ms_max / 1e3)
     nk = max(3, min(args.steps, 20))
     k = b.sweep_timed(nk, per_kernel=True)
     a_ms = float(k[1]) / nk
@@ -546,6 +589,8 @@ def bench_batched(args, dist: Dist, cp) -> dict:
         b.update_host_io(io)
         io.swap()
     e2e_s = dist.max(time.perf_counter() - t0)
+    # per-lattice observables of the final state, gathered on rank 0 (control plane only)
+    merged = shard.gather_results(mix_observables(b, ids, mine), dist.gather_object)
     b.close()
     res = {
         "value": value, "ms_per_step": ms_max / args.steps, "launches": launches, "clocks": clocks.summary(),
@@ -554,11 +599,16 @@ def bench_batched(args, dist: Dist, cp) -> dict:
                      "traffic": ASSIGN_TRAFFIC_PER_SITE["kb_assign"] * sites, "peak_kind": peak_kind,
                      "bytes_per_launch": ab, "ms_per_launch": a_ms},
         "kernels_ms_per_sweep": {"assign": a_ms, "merge": float(k[2]) / nk, "resolve_flip": float(k[3]) / nk},
-        "e2e": {"value": dist.world * sites * e2e_steps / e2e_s, "unit": "spin-updates/s",
-                "h2d_bytes_per_step": sites, "d2h_bytes_per_step": sites},
+        "e2e": {"value": sites_all * e2e_steps / e2e_s, "unit": "spin-updates/s",
+                "h2d_bytes_per_step": sites_all, "d2h_bytes_per_step": sites_all},
         "tiles": {str(L): [list(t), list(bl)] for (L, _, _), (t, bl) in sorted(zip(mix, tiles))},
         "autotune_table": table.get("device", "none"),
     }
+    if merged is not None:
+        n_all = [L * L for L, _, _ in mix_workload()]
+        res["shard"] = {"ranks": dist.world, "lattices_per_rank": [len(p) for p in parts],
+                        "bytes_imbalance": imbalance, "lattices_gathered": len(merged),
+                        "mean_E_per_site": float(np.mean([-merged[k][0] / n_all[k] for k in merged]))}
     if dist.world == 1 and not args.quick:
         pl = plain_loop(cp, mix, tiles, max(3, min(args.steps, 10)), dev)
         res["plain_loop"] = pl
@@ -567,42 +617,99 @@ def bench_batched(args, dist: Dist, cp) -> dict:
     return res
 
 
-def bench_serving(args, dist: Dist, cp) -> None:
-    """Continuous-batching serving: Poisson job arrivals at 10, 100 and 1000 per second, L
-    log-uniform in [32, 2048] (multiples of 16), T uniform in [1.5, 3.5], sweeps log-uniform in
-    [1e3, 1e5], a fixed 32 GB HBM budget; a bounded number of jobs per rate.  Reports job latency
-    percentiles, makespan and throughput per rate, and the same jobs of the first rate served one
-    at a time on the single-lattice path as the baseline.  Prints its own JSON line (rank 0)."""
-    from computational_physics_b200 import serving
-    n_jobs = max(8, min(args.steps, 48))
+def plain_subrecord(cp, dev: int, name: str = "plain16384", sweeps: int = 100) -> dict:
+    """One single-lattice workload beside the headline: ms per sweep, per-kernel ms and the
+    fraction of the HBM roofline by the algorithmic bytes per sweep (17.1 B/site at 16 x 8)."""
+    p = PLAIN[name]
+    L, tile, W, T = p["L"], p["tile"], p["W"], p["T"]
+    n = L * L
+    with cp.SwendsenWang2D(L, L, tile, W, seed_base=1, device=dev) as sw:
+        sw.hot_start(1)
+        sw.update(T, 5)
+        sw.synchronize()
+        ms = float(sw.sweep_timed(T, sweeps)[0]) / sweeps
+        k = sw.sweep_timed(T, 20, per_kernel=True) / 20
+        n_tiles, _ = sw.rng_shape()
+    peak, peak_kind = hbm_peak()
+    # algorithmic bytes per sweep: 11 B per site (spins and labels) plus every tile's lcg32 state
+    # (3 W + 1 words) read and written in each of the two phases that draw
+    sweep_bytes = n * 11 + n_tiles * 4 * (12 * W + 4)
+    return {"workload": name, "sites": n, "ms_per_sweep": ms, "value": n / (ms / 1e3),
+            "kernels_ms": {"assign": float(k[1]), "merge": float(k[2]), "resolve_flip": float(k[3])},
+            "bytes_per_sweep": sweep_bytes, "hbm_frac": sweep_bytes / (ms / 1e3) / 1e9 / peak, "peak": peak,
+            "peak_kind": peak_kind}
+
+
+SERVING_RATES = (10.0, 100.0, 1000.0)
+SERVING_JOBS = 200            # jobs per rate
+SERVING_BASELINE_JOBS = 40    # the first jobs of the stream, one at a time on the single-lattice path
+SERVING_SEED = 20260
+
+
+def serving_run(dist: Dist, n_jobs: int = SERVING_JOBS, baseline_jobs: int = SERVING_BASELINE_JOBS) -> dict:
+    """Continuous-batching serving of one job set (L log-uniform in [32, 2048] rounded to 16, T
+    uniform in [1.5, 3.5], sweeps log-uniform in [1e3, 1e5], a seed per job) arriving as a
+    Poisson stream at 10, 100 and 1000 jobs per second, under a 32 GB HBM budget per GPU.
+    Sharded: every job is served by one rank (partition by site updates); job records are
+    gathered on rank 0, which gets the summary (other ranks: None).  The baseline serves the
+    first `baseline_jobs` jobs one at a time on the single-lattice path, back to back."""
+    from computational_physics_b200 import serving, shard
     per_rate = {}
     work = span = 0.0
+    for rate in SERVING_RATES:
+        jobs = serving.poisson_jobs(rate, n_jobs, seed=SERVING_SEED)
+        mine = shard.shard_of([j.site_updates for j in jobs], dist.world, dist.rank)
+        local = [jobs[k] for k in mine]
+        srv = serving.Server(32 << 30, device=dist.local_rank)
+        try:
+            srv.run(local, realtime=True)
+        finally:
+            srv.close()
+        recs = {j.jid: [j.arrival, j.admitted, j.done, j.site_updates, j.result.get("z")] for j in local}
+        merged = shard.gather_results(recs, dist.gather_object)
+        rejected = dist.gather_object(len(srv.rejected))
+        bypassed = dist.gather_object(srv.bypassed)
+        if merged is None:
+            continue
+        for j in jobs:
+            j.arrival, j.admitted, j.done = merged[j.jid][0], merged[j.jid][1], merged[j.jid][2]
+        summ = serving.latency_summary(jobs)
+        zs = np.array([merged[k][4] for k in merged if merged[k][4] is not None and np.isfinite(merged[k][4])])
+        summ.update(rejected=int(sum(rejected)), bypassed=int(sum(bypassed)),
+                    jobs_within_2sigma=float(np.mean(np.abs(zs) <= 2)) if len(zs) else None)
+        per_rate[str(int(rate))] = summ
+        work += sum(j.site_updates for j in jobs if j.done is not None)
+        span += summ.get("makespan_s", 0.0)
+    base = None
+    if dist.rank == 0:
+        base_jobs = serving.poisson_jobs(SERVING_RATES[0], n_jobs, seed=SERVING_SEED)[:baseline_jobs]
+        t0 = time.perf_counter()
+        serving.SequentialServer(device=dist.local_rank).run(base_jobs, realtime=False)
+        secs = time.perf_counter() - t0
+        base = {"jobs": len(base_jobs), "site_updates_per_s": sum(j.site_updates for j in base_jobs) / secs,
+                "seconds": secs, "timing": "the first jobs of the same stream, back to back, host wall clock"}
+    if dist.rank != 0:
+        return None
+    return {"per_rate": per_rate, "value": work / span if span else 0.0, "sequential_baseline": base,
+            "jobs_per_rate": n_jobs, "ranks": dist.world}
+
+
+def bench_serving(args, dist: Dist, cp) -> None:
+    """The serving workload on its own (serving_run); prints its own JSON line (rank 0)."""
     with ClockSampler(dist.local_rank) as clocks:
-        for k, rate in enumerate((10.0, 100.0, 1000.0)):
-            jobs = serving.poisson_jobs(rate, n_jobs, seed=20260 + k)
-            srv = serving.Server(32 << 30, device=dist.local_rank)
-            try:
-                srv.run(jobs, realtime=True)
-            finally:
-                srv.close()
-            s = serving.latency_summary(jobs)
-            s["rejected"] = len(srv.rejected)
-            per_rate[str(int(rate))] = s
-            work += sum(j.site_updates for j in jobs if j.done is not None)
-            span += s.get("makespan_s", 0.0)
-        base_jobs = serving.poisson_jobs(10.0, n_jobs, seed=20260)
-        serving.SequentialServer(device=dist.local_rank).run(base_jobs, realtime=True)
-        base = serving.latency_summary(base_jobs)
+        r = serving_run(dist)
     if dist.rank != 0:
         return
+    n = r["jobs_per_rate"]
+    span = sum(v.get("makespan_s", 0.0) for v in r["per_rate"].values())
     print(json.dumps({
-        "metric": "SW spin-updates/s", "value": work / span, "unit": "spin-updates/s", "n_gpus": dist.world,
-        "steps": n_jobs, "warmup": 0, "ms_per_step": 1e3 * span / (3 * n_jobs), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "metric": "SW spin-updates/s", "value": r["value"], "unit": "spin-updates/s", "n_gpus": dist.world,
+        "steps": n, "warmup": 0, "ms_per_step": 1e3 * span / (len(SERVING_RATES) * n), "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
         "config": {"workload": "serving: Poisson arrivals at 10/100/1000 per s, L log-uniform [32, 2048], "
-                               "T uniform [1.5, 3.5], sweeps log-uniform [1e3, 1e5], 32 GB HBM budget",
-                   "jobs_per_rate": n_jobs, "parallelism": f"replicas x{dist.world}"},
-        "serving": per_rate, "sequential_baseline_rate10": base, "clocks": clocks.summary(),
+                               "T uniform [1.5, 3.5], sweeps log-uniform [1e3, 1e5], 32 GB HBM budget per GPU",
+                   "jobs_per_rate": n, "parallelism": f"job shards x{dist.world}"},
+        "serving": r["per_rate"], "sequential_baseline": r["sequential_baseline"], "clocks": clocks.summary(),
     }))
 
 
@@ -639,14 +746,22 @@ def main() -> None:
         line = {
             "metric": "SW spin-updates/s", "value": r["value"], "unit": "spin-updates/s", "n_gpus": dist.world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-            "config": {**workload_config(args.workload), "parallelism": f"replicas x{dist.world}"},
+            "scaling": "strong" if args.workload == "batched" else "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic",
+            "config": {**workload_config(args.workload),
+                       "parallelism": (f"lattice shards x{dist.world}" if args.workload == "batched"
+                                       else f"replicas x{dist.world}")},
             "roofline": r["roofline"], "e2e": r["e2e"], "gpu_launches": r["launches"], "clocks": r["clocks"],
             "kernels_ms_per_sweep": r["kernels_ms_per_sweep"],
         }
-        for key in ("plain_loop", "batched_vs_plain_loop", "energy_gate", "tiles", "autotune_table"):
+        for key in ("plain_loop", "batched_vs_plain_loop", "energy_gate", "tiles", "autotune_table", "shard"):
             if key in r:
                 line[key] = r[key]
+        if args.workload == "batched" and dist.world == 1 and not args.quick:
+            line["plain16384"] = plain_subrecord(cp, dist.local_rank)
+            sv = serving_run(dist)
+            line["serving"] = {"value": sv["value"], "unit": "spin-updates/s", "per_rate": sv["per_rate"],
+                               "sequential_baseline": sv["sequential_baseline"], "jobs_per_rate": sv["jobs_per_rate"]}
         if dist.world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args.workload)
         print(json.dumps(line))

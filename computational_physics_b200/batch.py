@@ -22,10 +22,13 @@ extra_signatures({
     "swb_batch_status": ([P, U32, P, P], I32),
     "swb_batch_poll": ([P, P, P], I32),
     "swb_batch_sweep": ([P, U32, I32], I32),
+    "swb_batch_mark": ([P, P], I32),
+    "swb_batch_mark_query": ([P, U32, P, P], I32),
     "swb_batch_synchronize": ([P], I32),
     "swb_batch_sweep_timed": ([P, U32, I32, P], I32),
     "swb_batch_accumulators": ([P, U32, P], I32),
     "swb_batch_samples": ([P, U32, P, U64, P], I32),
+    "swb_batch_samples_finished": ([P, U32, P, U64, P, P], I32),
     "swb_batch_get_rng": ([P, U32, P, P, P, P], I32),
     "swb_batch_set_rng": ([P, U32, P, P, P, P], I32),
     "swb_batch_info": ([P, U32, P], I32),
@@ -128,6 +131,20 @@ class BatchedSW:
     def sweep(self, rounds: int = 1, measure: bool = False) -> None:
         check(self._lib.swb_batch_sweep(self._h, rounds, int(measure)))
 
+    def mark(self) -> int:
+        """Records a point after the work submitted so far; see :meth:`mark_done`."""
+        m = ctypes.c_uint32()
+        check(self._lib.swb_batch_mark(self._h, ctypes.byref(m)))
+        return m.value
+
+    def mark_done(self, mark: int) -> float | None:
+        """None while the device has not passed `mark`, else its device time in seconds since
+        the first mark (non-blocking)."""
+        done = ctypes.c_int()
+        ms = ctypes.c_double()
+        check(self._lib.swb_batch_mark_query(self._h, mark, ctypes.byref(done), ctypes.byref(ms)))
+        return ms.value / 1e3 if done.value else None
+
     def synchronize(self) -> None:
         check(self._lib.swb_batch_synchronize(self._h))
 
@@ -147,6 +164,14 @@ class BatchedSW:
         out = np.empty((n.value, 2), np.int64)
         check(self._lib.swb_batch_samples(self._h, lid, _ptr(out), n.value, ctypes.byref(n)))
         return out
+
+    def samples_finished(self, lid: int, max_samples: int) -> np.ndarray:
+        """The sample series of a lattice that has finished its sweep budget, read without
+        waiting for the batch's other work (valid once a mark after its last sweep is passed)."""
+        n = ctypes.c_uint64()
+        out = np.empty((max_samples, 2), np.int64)
+        check(self._lib.swb_batch_samples_finished(self._h, lid, _ptr(out), max_samples, ctypes.byref(n), None))
+        return out[:min(n.value, max_samples)]
 
     def get_rng(self, lid: int):
         g = self.info(lid)

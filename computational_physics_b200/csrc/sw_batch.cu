@@ -51,7 +51,7 @@ struct BatchLat {
     uint32_t swept;           // 1 if this lattice was swept in the current round
     uint32_t measure_every;   // measure after every measure_every-th sweep (0: never)
     uint32_t sweeps_done;     // sweeps completed
-    uint32_t blocks_left;     // flip work items not yet done in this round
+    uint32_t pad;
 };
 
 struct BatchCounters {
@@ -145,8 +145,7 @@ __global__ void __launch_bounds__(kMergeThreads) kb_resolve(BatchLat *lats, cons
     }
 }
 
-// Flip of one block (flip_block, after kb_resolve); the last block of a lattice closes its
-// round (sweep count and budget).
+// Flip of one block (flip_block, after kb_resolve).
 __global__ void __launch_bounds__(kFlipThreads, 6) kb_flip(BatchLat *lats, const uint2 *items, const uint32_t total,
                                                             unsigned int *fault)
 {
@@ -154,23 +153,31 @@ __global__ void __launch_bounds__(kFlipThreads, 6) kb_flip(BatchLat *lats, const
     uint2 d = load_item(items, blockIdx.x, total);
     for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
         const uint2 next = load_item(items, item + gridDim.x, total);
-        BatchLat *L = lats + d.x;
+        const BatchLat *L = lats + d.x;
         if (L->sweeps_left != 0) {
             const Geo g = L->g;
             flip_block<false, 4, true>(g, d.y & 0xFFFFu, d.y >> 16, L->spins, L->labels, fault, smem);
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                __threadfence();
-                if (atomicSub(&L->blocks_left, 1u) == 1u) {
-                    L->blocks_left = g.nbx * g.nby;
-                    L->swept = 1;
-                    L->sweeps_done += 1;
-                    if (L->sweeps_left != kUnlimited)
-                        L->sweeps_left -= 1;
-                }
-            }
+            if (item + gridDim.x < total)
+                __syncthreads();  // the next item reuses the shared memory
         }
         d = next;
+    }
+}
+
+// Closes a round after every phase kernel of it (before the measurement): each lattice that was
+// swept counts the sweep and spends one from its budget.  The kernels of the round read the
+// budget only to skip finished lattices, so it changes here, between rounds.
+__global__ void kb_end_round(BatchLat *lats, const uint32_t *active, const BatchCounters *ctr)
+{
+    const uint32_t n = ctr->n_active;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        BatchLat *L = lats + active[k];
+        if (L->sweeps_left != 0) {
+            L->swept = 1;
+            L->sweeps_done += 1;
+            if (L->sweeps_left != kUnlimited)
+                L->sweeps_left -= 1;
+        }
     }
 }
 
@@ -376,6 +383,9 @@ struct swb_batch {
     } io;
     std::vector<cudaEvent_t> io_events;
     std::vector<uint32_t> active;   // ids in the work lists
+    cudaEvent_t origin = nullptr;           // swb_batch_mark's time origin (recorded at the first mark)
+    std::vector<cudaEvent_t> marks;         // swb_batch_mark's events, a ring
+    uint32_t next_mark = 0;
     bool lists_dirty = true;
     int grid_measure = 0;
     uint32_t smem_assign = 0, smem_flip = 0;
@@ -409,7 +419,7 @@ uint64_t lattice_bytes(const Geo &g, uint32_t W, uint64_t series_cap)
 {
     const uint64_t n = (uint64_t)g.L0 * g.L1, tiles = (uint64_t)g.n0 * g.n1, blocks = (uint64_t)g.nbx * g.nby;
     auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
-    return al(n) + al(4 * n) + al(4 * tiles * W) + al(tiles * W) + al(4 * tiles) + al(4 * kEdgeWords * blocks) +
+    return al(n) + al(4 * n) + al(4 * tiles * W) + al(tiles * W) + al(4 * tiles) + al(4 * (uint64_t)edge_stride(g) * blocks) +
            al(4 * (uint64_t)(g.BX + g.BY) * blocks) + al(sizeof(Obs)) + al(16 * series_cap);
 }
 
@@ -545,6 +555,22 @@ int launch_phases_b(swb_batch *b, const uint2 *items, uint32_t n, cudaStream_t s
     return launch_flip_b(b, items, n, st);
 }
 
+int launch_end_round(swb_batch *b, cudaStream_t st)
+{
+    kb_end_round<<<4, 128, 0, st>>>(b->d_lats, b->d_active, b->d_ctr);
+    SWB_LAUNCHED();
+    return SWB_OK;
+}
+
+// Kernels of one captured round: begin, four phases per non-empty lattice group, end, measure.
+uint32_t round_launches(const swb_batch *b, bool measure)
+{
+    uint32_t n = 2 + (measure ? 1 : 0);
+    for (uint32_t q = 0; q < kRoundGroups; ++q)
+        n += b->grp_count[q] ? 4 : 0;
+    return n;
+}
+
 int launch_round(swb_batch *b, bool measure)
 {
     kb_begin_round<<<4, 128, 0, b->stream>>>(b->d_lats, b->d_active, b->d_ctr);
@@ -569,6 +595,8 @@ int launch_round(swb_batch *b, bool measure)
         SWB_CUDA(cudaEventRecord(b->join[q], b->gstream[q]));
         SWB_CUDA(cudaStreamWaitEvent(b->stream, b->join[q], 0));
     }
+    if (int rc = launch_end_round(b, b->stream))
+        return rc;
     if (measure) {
         kb_measure<<<b->grid_measure, kBatchThreads, 0, b->stream>>>(b->d_lats, b->d_active, b->d_chunk_prefix,
                                                                    b->d_ctr);
@@ -626,7 +654,7 @@ int rounds(swb_batch *b, uint32_t n_rounds, bool any_measure)
         return rc;
     for (uint32_t r = 0; r < n_rounds; ++r) {
         SWB_CUDA(cudaGraphLaunch(ge, b->stream));
-        g_launches.fetch_add(any_measure ? 5 : 4, std::memory_order_relaxed);
+        g_launches.fetch_add(round_launches(b, any_measure), std::memory_order_relaxed);
     }
     return SWB_OK;
 }
@@ -725,6 +753,10 @@ int swb_batch_destroy(swb_batch *b)
         if (b->gstream[q])
             cudaStreamDestroy(b->gstream[q]);
     }
+    for (auto e : b->marks)
+        cudaEventDestroy(e);
+    if (b->origin)
+        cudaEventDestroy(b->origin);
     if (b->s_in)
         cudaStreamDestroy(b->s_in);
     if (b->s_out)
@@ -782,7 +814,7 @@ int swb_batch_add(swb_batch *b, uint32_t L0, uint32_t L1, uint32_t tile_x, uint3
     d.rng_state = reinterpret_cast<uint32_t *>(p); p += al(4 * tiles * b->W);
     d.rng_sel = reinterpret_cast<uint8_t *>(p); p += al(tiles * b->W);
     d.rng_iter = reinterpret_cast<uint32_t *>(p); p += al(4 * tiles);
-    d.edge = reinterpret_cast<uint32_t *>(p); p += al(4 * kEdgeWords * blocks);
+    d.edge = reinterpret_cast<uint32_t *>(p); p += al(4 * (uint64_t)edge_stride(g) * blocks);
     d.linked = reinterpret_cast<uint32_t *>(p); p += al(4 * (uint64_t)(g.BX + g.BY) * blocks);
     d.obs = reinterpret_cast<Obs *>(p); p += al(sizeof(Obs));
     d.series = reinterpret_cast<long long *>(p);
@@ -790,7 +822,6 @@ int swb_batch_add(swb_batch *b, uint32_t L0, uint32_t L1, uint32_t tile_x, uint3
     d.thr = accept_threshold(swb_p_add(temperature));
     d.sweeps_left = kUnlimited;
     d.measure_every = 0;
-    d.blocks_left = g.nbx * g.nby;
     SWB_CUDA(cudaMemsetAsync(d.spins, 0, n, b->stream));
     SWB_CUDA(cudaMemsetAsync(d.obs, 0, sizeof(Obs), b->stream));
     switch (b->W) {
@@ -940,6 +971,51 @@ int swb_batch_sweep(swb_batch *b, uint32_t n_rounds, int measure)
     return rounds(b, n_rounds, measure != 0);
 }
 
+constexpr uint32_t kMarks = 64;  // marks in flight at once
+
+int swb_batch_mark(swb_batch *b, uint32_t *mark)
+{
+    if (!b || !mark)
+        return fail(SWB_ERR_ARGUMENT, "NULL argument");
+    if (int rc = bset_device(b))
+        return rc;
+    if (!b->origin) {
+        SWB_CUDA(cudaEventCreate(&b->origin));
+        SWB_CUDA(cudaEventRecord(b->origin, b->stream));
+        b->marks.assign(kMarks, nullptr);
+        for (auto &e : b->marks)
+            SWB_CUDA(cudaEventCreate(&e));
+    }
+    const uint32_t m = b->next_mark++;
+    SWB_CUDA(cudaEventRecord(b->marks[m % kMarks], b->stream));
+    *mark = m;
+    return SWB_OK;
+}
+
+int swb_batch_mark_query(swb_batch *b, uint32_t mark, int *done, double *ms)
+{
+    if (!b || !done)
+        return fail(SWB_ERR_ARGUMENT, "NULL argument");
+    if (!b->origin || mark >= b->next_mark || b->next_mark - mark > kMarks)
+        return fail(SWB_ERR_ARGUMENT, "mark %u is not one of the last %u marks", mark, kMarks);
+    if (int rc = bset_device(b))
+        return rc;
+    cudaEvent_t e = b->marks[mark % kMarks];
+    const cudaError_t q = cudaEventQuery(e);
+    if (q == cudaErrorNotReady) {
+        *done = 0;
+        return SWB_OK;
+    }
+    SWB_CUDA(q);
+    *done = 1;
+    if (ms) {
+        float t = 0.0f;
+        SWB_CUDA(cudaEventElapsedTime(&t, b->origin, e));
+        *ms = t;
+    }
+    return SWB_OK;
+}
+
 int swb_batch_synchronize(swb_batch *b)
 {
     if (!b)
@@ -983,6 +1059,8 @@ int swb_batch_sweep_timed(swb_batch *b, uint32_t n_rounds, int per_kernel, float
             if ((rc = launch_flip_b(b, b->d_items, b->items_n, b->stream)))
                 break;
             SWB_CUDA(cudaEventRecord(ev[4], b->stream));
+            if ((rc = launch_end_round(b, b->stream)))
+                break;
             SWB_CUDA(cudaEventSynchronize(ev[4]));
             float t;
             SWB_CUDA(cudaEventElapsedTime(&t, ev[1], ev[2]));
@@ -1015,6 +1093,32 @@ int swb_batch_accumulators(swb_batch *b, uint32_t id, double *out)
     return SWB_OK;
 }
 
+namespace {
+
+// The sample series of lattice h, read on stream st (waited for) after the work already
+// ordered before it there.
+int read_samples(swb_batch *b, HostLat *h, cudaStream_t st, int64_t *em, uint64_t capacity, uint64_t *count,
+                 double *acc)
+{
+    Obs o;
+    SWB_CUDA(cudaMemcpyAsync(&o, h->d.obs, sizeof(o), cudaMemcpyDeviceToHost, st));
+    SWB_CUDA(cudaStreamSynchronize(st));
+    *count = o.n_samples;
+    if (acc)
+        std::memcpy(acc, o.acc, sizeof(o.acc));
+    if (o.n_samples > h->d.series_cap)
+        return fail(SWB_ERR_CAPACITY, "%llu samples recorded, series keeps %llu", o.n_samples, h->d.series_cap);
+    const uint64_t k = std::min<uint64_t>(o.n_samples, capacity);
+    if (k && em) {
+        SWB_CUDA(cudaMemcpyAsync(em, h->d.series, k * 16, cudaMemcpyDeviceToHost, st));
+        SWB_CUDA(cudaStreamSynchronize(st));
+    }
+    (void)b;
+    return SWB_OK;
+}
+
+}  // namespace
+
 int swb_batch_samples(swb_batch *b, uint32_t id, int64_t *em, uint64_t capacity, uint64_t *count)
 {
     HostLat *h = get_lat(b, id);
@@ -1022,18 +1126,20 @@ int swb_batch_samples(swb_batch *b, uint32_t id, int64_t *em, uint64_t capacity,
         return fail(SWB_ERR_ARGUMENT, "no lattice %u or NULL count", id);
     if (int rc = bset_device(b))
         return rc;
-    Obs o;
-    SWB_CUDA(cudaMemcpyAsync(&o, h->d.obs, sizeof(o), cudaMemcpyDeviceToHost, b->stream));
-    SWB_CUDA(cudaStreamSynchronize(b->stream));
-    *count = o.n_samples;
-    if (o.n_samples > h->d.series_cap)
-        return fail(SWB_ERR_CAPACITY, "%llu samples recorded, series keeps %llu", o.n_samples, h->d.series_cap);
-    const uint64_t k = std::min<uint64_t>(o.n_samples, capacity);
-    if (k && em) {
-        SWB_CUDA(cudaMemcpyAsync(em, h->d.series, k * 16, cudaMemcpyDeviceToHost, b->stream));
-        SWB_CUDA(cudaStreamSynchronize(b->stream));
-    }
-    return SWB_OK;
+    return read_samples(b, h, b->stream, em, capacity, count, nullptr);
+}
+
+int swb_batch_samples_finished(swb_batch *b, uint32_t id, int64_t *em, uint64_t capacity, uint64_t *count,
+                               double *acc)
+{
+    HostLat *h = get_lat(b, id);
+    if (!h || !count)
+        return fail(SWB_ERR_ARGUMENT, "no lattice %u or NULL count", id);
+    if (int rc = bset_device(b))
+        return rc;
+    if (!b->s_out)
+        SWB_CUDA(cudaStreamCreateWithFlags(&b->s_out, cudaStreamNonBlocking));
+    return read_samples(b, h, b->s_out, em, capacity, count, acc);
 }
 
 int swb_batch_get_rng(swb_batch *b, uint32_t id, uint32_t *state, uint32_t *a, uint32_t *c, uint32_t *iteration)
@@ -1241,6 +1347,9 @@ int swb_batch_update_host(swb_batch *b, uint32_t count, const uint32_t *ids, con
                 return rc;
             kb_stage_copy<<<n, 512, 0, b->stream>>>(b->d_copies + gs[g], b->d_stage, 0);
             SWB_LAUNCHED();
+            if (g + 1 == G)  // every listed and unlisted lattice has swept: close the round
+                if (int rc = launch_end_round(b, b->stream))
+                    return rc;
             SWB_CUDA(cudaEventRecord(ev[G + g], b->stream));
             SWB_CUDA(cudaStreamWaitEvent(b->s_out, ev[G + g], 0));
             for (uint32_t k = gs[g]; k < gs[g + 1];) {

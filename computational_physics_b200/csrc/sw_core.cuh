@@ -23,9 +23,10 @@ extern std::atomic<uint64_t> g_launches;
 int fail(int code, const char *fmt, ...);
 
 // swb_sweep_static's scratch: one file-scope device array (sw_static_scratch.cu) holding the
-// label array, the block edge words and the fault word of a lattice of at most 2048 x 2048 sites.
+// label array, the block edge records and the fault word of a lattice of at most 2048 x 2048
+// sites: 16 MiB of labels plus at most 2.2 bytes per site of edge records (tile 8 x 2).
 constexpr uint64_t kStaticMaxSites = 1ull << 22;               // 2048 x 2048 sites
-constexpr size_t kStaticScratchBytes = (24ull << 20) + 1024;   // labels 16 MiB + edge words + fault
+constexpr size_t kStaticScratchBytes = 26ull << 20;            // 26 MiB
 // Device address of that array on `device`, which must be current (looked up once per device).
 int static_scratch_base(int device, unsigned char **base);
 
@@ -192,6 +193,40 @@ struct AssignDump {
     uint32_t *block_labels;
     uint32_t *tile_labels;
 };
+
+// The per-block edge record: kEdgeWords bond words ([0] the right edge's bonds by row, [1..4]
+// the bottom edge's by column), then the global root index of every site on the block's four
+// edges, written by the assign phase so that the merge reads them coalesced instead of
+// gathering label columns: right column [BY], left column [BY], bottom row [BX], top row [BX].
+__host__ __device__ inline uint32_t edge_stride(const Geo &g) { return kEdgeWords + 2 * (g.BX + g.BY); }
+
+// Fills the root part of block (bxi, byi)'s edge record, one slot per thread: root(l) gives the
+// block-local index of the root of block-local site l (its component's minimum).
+template <class Root>
+__device__ __forceinline__ void edge_roots(const Geo &g, const uint32_t bxi, const uint32_t byi, uint32_t *__restrict__ er,
+                                           const Root &root)
+{
+    const uint32_t BX = g.BX, BY = g.BY, x0 = bxi * BX, y0 = byi * BY;
+    const uint32_t bxv = min(BX, g.L0 - x0), byv = min(BY, g.L1 - y0);
+    for (uint32_t i = threadIdx.x; i < 2 * (BX + BY); i += blockDim.x) {
+        uint32_t xl, yl;
+        if (i < 2 * BY) {  // right column, then left column
+            yl = i < BY ? i : i - BY;
+            xl = i < BY ? bxv - 1 : 0;
+            if (yl >= byv)
+                continue;
+        } else {           // bottom row, then top row
+            const uint32_t j = i - 2 * BY;
+            xl = j < BX ? j : j - BX;
+            yl = j < BX ? byv - 1 : 0;
+            if (xl >= bxv)
+                continue;
+        }
+        const uint32_t r = root(yl * BX + xl);
+        const uint32_t ry = (BX & (BX - 1)) == 0 ? r >> (__ffs(BX) - 1) : r / BX;  // BX: a power of two but
+        er[kEdgeWords + i] = (y0 + ry) * g.L0 + x0 + (r - ry * BX);               // where the caller chose it
+    }
+}
 
 struct AssignSmem {
     uint32_t parent, draws, slots, edge, bond, sp, plab, total, pitch;
@@ -523,8 +558,10 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
             }
         }
     }
+    uint32_t *erec = edge + ((size_t)byi * g.nbx + bxi) * edge_stride(g);  // this block's edge record
+    edge_roots(g, bxi, byi, erec, [&](uint32_t l) { return uf_find_halve(parent, plab[l]); });
     if (tid < kEdgeWords)
-        edge[((size_t)byi * g.nbx + bxi) * kEdgeWords + tid] = edge_s[tid];
+        erec[tid] = edge_s[tid];
     if (meas.obs && tid == 0)  // the block's sums (complete since the barrier after the bond words)
         obs_add_part(meas.obs, meas.series, meas.cap, (size_t)g.L0 * g.L1, g.nbx * g.nby,
                      reinterpret_cast<const int *>(edge_s)[kEdgeE], reinterpret_cast<const int *>(edge_s)[kEdgeM], 1);
@@ -850,8 +887,10 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
                 dump.block_labels[(size_t)(y0 + yl) * g.L0 + x0 + xl] = (y0 + r / BX) * g.L0 + x0 + r % BX;
         }
     }
+    edge_roots(g, bxi, byi, edge + ((size_t)byi * g.nbx + bxi) * edge_stride(g),
+               [&](uint32_t l) { return uf_find(parent, l); });
     if (tid < kEdgeWords)
-        edge[((size_t)byi * g.nbx + bxi) * kEdgeWords + tid] = edge_s[tid];
+        edge[((size_t)byi * g.nbx + bxi) * edge_stride(g) + tid] = edge_s[tid];
 }
 
 // assign_block with the tile shape as compile-time constants for the common shapes (lcg width
@@ -893,33 +932,30 @@ __device__ __forceinline__ void merge_block(const Geo &g, const uint32_t bxi, co
 {
     const uint32_t x0 = bxi * g.BX, y0 = byi * g.BY;
     const uint32_t bxv = min(g.BX, g.L0 - x0), byv = min(g.BY, g.L1 - y0);
-    const uint32_t *e = edge + ((size_t)byi * g.nbx + bxi) * kEdgeWords;
-    size_t s = 0, nb = 0;
-    uint32_t nbx = bxi, nby = byi;  // block of the neighbour site
+    const uint32_t es = edge_stride(g);
+    const uint32_t *e = edge + ((size_t)byi * g.nbx + bxi) * es;
+    uint32_t a = 0, b = 0;
     bool go = false;
     if (t < g.BY) {
-        if (t < byv && ((e[0] >> t) & 1u)) {
-            s = (size_t)(y0 + t) * g.L0 + x0 + bxv - 1;
-            nb = (size_t)(y0 + t) * g.L0 + (x0 + bxv < g.L0 ? x0 + bxv : 0u);
-            nbx = bxi + 1 == g.nbx ? 0 : bxi + 1;
+        if (t < byv && ((e[0] >> t) & 1u)) {  // this block's right column, the next block's left column
+            const uint32_t nbx = bxi + 1 == g.nbx ? 0 : bxi + 1;
+            a = e[kEdgeWords + t];
+            b = edge[((size_t)byi * g.nbx + nbx) * es + kEdgeWords + g.BY + t];
             go = true;
         }
     } else {
         const uint32_t xl = t - g.BY;
-        if (xl < bxv && ((e[1 + (xl >> 5)] >> (xl & 31)) & 1u)) {
-            s = (size_t)(y0 + byv - 1) * g.L0 + x0 + xl;
-            nb = (size_t)(y0 + byv < g.L1 ? y0 + byv : 0u) * g.L0 + x0 + xl;
-            nby = byi + 1 == g.nby ? 0 : byi + 1;
+        if (xl < bxv && ((e[1 + (xl >> 5)] >> (xl & 31)) & 1u)) {  // this block's bottom row, the top row below
+            const uint32_t nby = byi + 1 == g.nby ? 0 : byi + 1;
+            a = e[kEdgeWords + 2 * g.BY + xl];
+            b = edge[((size_t)nby * g.nbx + bxi) * es + kEdgeWords + 2 * g.BY + g.BX + xl];
             go = true;
         }
     }
+    (void)x0; (void)y0;
     uint32_t link = kNoLink;
-    if (go) {
-        const volatile uint32_t *vl = labels;
-        const uint32_t a = label_global(g, bxi, byi, vl[s]), b = label_global(g, nbx, nby, vl[nb]);
-        if (a != b)
-            link = guf_union_pair(labels, a, b, fault);
-    }
+    if (go && a != b)
+        link = guf_union_pair(labels, a, b, fault);
     if (linked)
         linked[((size_t)byi * g.nbx + bxi) * (g.BX + g.BY) + t] = link;
 }

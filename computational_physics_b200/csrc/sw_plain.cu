@@ -489,7 +489,7 @@ int swb_create(swb_lattice **out, uint32_t L0, uint32_t L1, uint32_t tile_x, uin
     SWB_TRY(cudaMalloc(&h->rng_state, (size_t)h->n_tiles * h->W * sizeof(uint32_t)));
     SWB_TRY(cudaMalloc(&h->rng_sel, (size_t)h->n_tiles * h->W));
     SWB_TRY(cudaMalloc(&h->rng_iter, (size_t)h->n_tiles * sizeof(uint32_t)));
-    SWB_TRY(cudaMalloc(&h->edge, (size_t)h->n_blocks * kEdgeWords * sizeof(uint32_t)));
+    SWB_TRY(cudaMalloc(&h->edge, (size_t)h->n_blocks * edge_stride(h->g) * sizeof(uint32_t)));
     bool resolve = h->n_blocks >= kResolveMinBlocks || h->g.BX * h->g.BY >= kResolveBlockSites;
     if (const char *e = std::getenv("SWB_RESOLVE_MIN_BLOCKS"))
         resolve = h->n_blocks >= (uint32_t)std::strtoul(e, nullptr, 10);
@@ -919,7 +919,9 @@ int swb_copy_to_device(int device, void *dst, const void *src, size_t bytes)
     if ((!dst || !src) && bytes)
         return fail(SWB_ERR_ARGUMENT, "NULL argument");
     SWB_CUDA(cudaSetDevice(device));
+    SWB_CUDA(cudaDeviceSynchronize());  // the engine's streams do not order against this copy
     SWB_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+    SWB_CUDA(cudaDeviceSynchronize());  // a copy from pageable memory may return before it lands
     return SWB_OK;
 }
 
@@ -928,6 +930,7 @@ int swb_copy_to_host(int device, void *dst, const void *src, size_t bytes)
     if ((!dst || !src) && bytes)
         return fail(SWB_ERR_ARGUMENT, "NULL argument");
     SWB_CUDA(cudaSetDevice(device));
+    SWB_CUDA(cudaDeviceSynchronize());  // the engine's streams do not order against this copy
     SWB_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
     return SWB_OK;
 }
@@ -959,6 +962,7 @@ int swb_spins_energy_magnetization(int device, uint32_t L0, uint32_t L1, const v
     static std::vector<Obs *> acc;
     std::lock_guard<std::mutex> lock(mu);
     SWB_CUDA(cudaSetDevice(device));
+    SWB_CUDA(cudaDeviceSynchronize());  // every sweep queued on the engine's streams comes first
     if ((int)acc.size() <= device)
         acc.resize(device + 1, nullptr);
     if (!acc[device]) {
@@ -1034,7 +1038,7 @@ int swb_update_host(swb_lattice *h, float temperature, const uint8_t *spins_in, 
 // pool already holds its whole HBM budget.  For such a caller a per-sweep cudaMalloc can fail
 // (the pool has the memory) and a cudaFree synchronises the whole device, stalling the other
 // lattices' streams.  The caller passes its spins and lcg32 streams; the sweep's scratch (label
-// array, block edge words, fault word) lives in the one file-scope device array below, which
+// array, block edge records, fault word) lives in one file-scope device array (sw_static_scratch.cu), which
 // every call on a device shares.
 
 namespace swb {
@@ -1079,7 +1083,7 @@ int swb_sweep_static(void *stream, uint32_t L0, uint32_t L1, uint32_t tile_x, ui
     h.smem_assign = assign_smem(h.g, h.W).total;
     h.smem_flip = flip_smem_bytes(h.g);
     const size_t labels_bytes = align256(h.n * sizeof(uint32_t) + 16);
-    const size_t edge_bytes = align256((size_t)h.n_blocks * kEdgeWords * sizeof(uint32_t));
+    const size_t edge_bytes = align256((size_t)h.n_blocks * edge_stride(h.g) * sizeof(uint32_t));
     if (labels_bytes + edge_bytes + 256 > kStaticScratchBytes)
         return fail(SWB_ERR_CAPACITY, "lattice %u x %u with tile %u x %u needs %zu bytes of scratch, the static array holds %zu",
                     L0, L1, tile_x, tile_y, labels_bytes + edge_bytes + 256, kStaticScratchBytes);
@@ -1096,7 +1100,7 @@ int swb_sweep_static(void *stream, uint32_t L0, uint32_t L1, uint32_t tile_x, ui
     h.edge = reinterpret_cast<uint32_t *>(base + labels_bytes);
     h.fault = reinterpret_cast<unsigned int *>(base + labels_bytes + edge_bytes);
 
-    // The array keeps the previous call's contents.  Labels and edge words are fully written by
+    // The array keeps the previous call's contents.  Labels and edge records are fully written by
     // the assign kernel before they are read; only the fault word must start at zero.
     SWB_CUDA(cudaMemsetAsync(h.fault, 0, sizeof(unsigned int), h.stream));
     const float p_add = swb_p_add(temperature);

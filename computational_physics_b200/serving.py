@@ -3,14 +3,20 @@
 A job is (L, T, sweeps, seed): an L x L periodic lattice hot-started from `seed`, swept
 `sweeps` times at temperature T with E and M measured every `measure_every` sweeps; its
 result is E/N (and |M|/N) averaged over the measurements after the first `discard` fraction,
-with a blocking error, plus the exact finite-lattice E/N.
+with a blocking error, plus the exact finite-lattice E/N, and the raw (e, m) series.
 
-:class:`Server` admits arriving jobs into a :class:`BatchedSW` as slots and HBM budget allow
-(first come, first served), keeps their spins, labels and lcg32 streams resident, and sweeps
-every admitted job together: a job that arrives while others run joins at the next round.
-Each job's sweep budget is counted on the device, so a job stops at exactly its sweep count
-and gives the same result as it would alone.  :class:`SequentialServer` is the baseline: jobs
-one at a time on the single-lattice path.
+:class:`Server` admits arriving jobs into a :class:`BatchedSW` as slots and HBM budget allow,
+keeps their spins, labels and lcg32 streams resident, and sweeps every admitted job together:
+a job that arrives while others run joins at the next round.  Each job's sweep budget is
+counted on the device, so a job stops at exactly its sweep count and gives the same result as
+it would alone.  The host loop never waits on the device to learn progress: every round
+sweeps every unfinished job once, so the host knows in which submitted round each job
+finishes, marks that point on the stream (swb_batch_mark) and learns its device completion
+time without blocking (swb_batch_mark_query); it keeps the next rounds queued meanwhile.
+Admission is first come, first served with a bounded bypass: when the head of the queue does
+not fit, up to `bypass_window` smaller waiting jobs behind it may go first, at most
+`max_bypass` times per head job.  :class:`SequentialServer` is the baseline: jobs one at a time
+on the single-lattice path.
 """
 from __future__ import annotations
 
@@ -54,9 +60,10 @@ class Job:
 def poisson_jobs(rate: float, n: int, seed: int = 0, L_range=(32, 2048), T_range=(1.5, 3.5),
                  sweeps_range=(1e3, 1e5)) -> list[Job]:
     """n jobs with Poisson arrivals at `rate` per second; L log-uniform in L_range rounded to a
-    multiple of 16, T uniform, sweeps log-uniform, one seed per job."""
+    multiple of 16, T uniform, sweeps log-uniform, one seed per job.  The same seed gives the
+    same jobs at every rate (only the arrival times scale with 1 / rate)."""
     rng = np.random.default_rng(seed)
-    t = np.cumsum(rng.exponential(1.0 / rate, size=n))
+    t = np.cumsum(rng.exponential(1.0, size=n)) / rate
     L = np.exp(rng.uniform(math.log(L_range[0]), math.log(L_range[1]), size=n))
     L = np.clip(np.round(L / 16) * 16, 16, None).astype(int)
     T = rng.uniform(*T_range, size=n)
@@ -70,7 +77,7 @@ def _result(samples: np.ndarray, L: int, T: float, discard: float) -> dict:
     k0 = int(len(samples) * discard)
     E = -samples[k0:, 0].astype(np.float64) / n
     M = np.abs(samples[k0:, 1].astype(np.float64)) / n
-    out = {"samples": int(len(samples)), "used": int(len(E)), "exact_E": exact_energy(T, L)}
+    out = {"samples": int(len(samples)), "used": int(len(E)), "exact_E": exact_energy(T, L), "series": samples}
     if len(E):
         b = binning_error(E, min_blocks=8)
         out.update({"E": b.mean, "E_err": b.error, "absM": float(M.mean()),
@@ -80,14 +87,19 @@ def _result(samples: np.ndarray, L: int, T: float, discard: float) -> dict:
 
 class Server:
     def __init__(self, hbm_budget_bytes: int, capacity: int = 1024, device: int = 0, measure_every: int = 10,
-                 discard: float = 0.1, target_round_ms: float = 2.0, max_rounds: int = 256):
+                 discard: float = 0.1, target_round_ms: float = 4.0, max_rounds: int = 512, bypass_window: int = 16,
+                 max_bypass: int = 64, max_in_flight: int = 2):
         self.batch = BatchedSW(capacity, hbm_budget_bytes, 16, device)
         self.measure_every = measure_every
         self.discard = discard
         self.target_ms = target_round_ms
         self.max_rounds = max_rounds
+        self.bypass_window = bypass_window
+        self.max_bypass = max_bypass
+        self.max_in_flight = max_in_flight
         self.table = autotune.load()
         self.rejected: list[Job] = []
+        self.bypassed = 0   # admissions that went ahead of a waiting head job
 
     def close(self):
         self.batch.close()
@@ -107,41 +119,94 @@ class Server:
     def run(self, jobs: list[Job], realtime: bool = True) -> list[Job]:
         """Serves `jobs` (arrival times relative to the start).  With realtime=False every job
         is treated as arrived at time 0."""
+        b = self.batch
         pending = deque(sorted(jobs, key=lambda j: j.arrival))
-        waiting: deque[Job] = deque()
-        running: dict[int, Job] = {}
-        round_ms = 1.0
+        waiting: list[Job] = []
+        running: dict[int, Job] = {}      # slot -> job still sweeping (host count of its rounds left)
+        left: dict[int, int] = {}         # slot -> rounds still to submit for its job
+        finishing: dict[int, list[int]] = {}  # mark -> slots whose last sweep precedes it
+        finished: list[int] = []          # slots done and read, memory not yet released
+        in_flight: deque[tuple[int, int]] = deque()  # (mark, rounds) submitted, not yet passed
+        head_skips = 0
+        rate = 1.0                        # rounds per ms, measured
         t0 = time.perf_counter()
         clock = lambda: time.perf_counter() - t0
-        while pending or waiting or running:
+        origin_mark = b.mark()            # device time origin ~ host time t_origin
+        t_origin = clock()
+        b.mark_done(origin_mark)
+        last_mark_time = (0.0, 0)          # (device s, rounds) of the last passed mark
+
+        def release_finished():
+            while finished:
+                b.remove(finished.pop())
+
+        while pending or waiting or running or in_flight:
             now = clock()
             while pending and (not realtime or pending[0].arrival <= now):
                 waiting.append(pending.popleft())
-            while waiting:
-                lid = self._admit(waiting[0])
-                if lid is None:
-                    if not running:  # too big for the budget even when the GPU is empty
-                        self.rejected.append(waiting.popleft())
-                        continue
+            # admission: the head first; up to bypass_window jobs behind it may go ahead when
+            # it does not fit, at most max_bypass times for one head
+            i = 0
+            while i < len(waiting) and i <= self.bypass_window:
+                if i > 0 and head_skips >= self.max_bypass:
                     break
-                job = waiting.popleft()
+                lid = self._admit(waiting[i])
+                if lid is None and finished:
+                    release_finished()
+                    lid = self._admit(waiting[i])
+                if lid is None:
+                    if i == 0 and not running and not in_flight:
+                        self.rejected.append(waiting.pop(0))  # too big even for an empty GPU
+                        continue
+                    i += 1
+                    continue
+                job = waiting.pop(i)
+                if i > 0:
+                    head_skips += 1
+                    self.bypassed += 1
+                else:
+                    head_skips = 0
                 job.admitted = clock()
                 running[lid] = job
-            if not running:
-                if pending:
-                    time.sleep(max(0.0, min(pending[0].arrival - clock(), 0.01)))
+                left[lid] = job.sweeps
+            # keep up to max_in_flight submissions queued: rounds until the next job finishes,
+            # fewer when an arrival is due sooner
+            if running and len(in_flight) < self.max_in_flight and any(left[l] for l in running):
+                r = min(left[l] for l in running if left[l])
+                cap = self.max_rounds
+                if pending and realtime:
+                    cap = max(1, int(rate * 1e3 * max(pending[0].arrival - now, 0.0)))
+                r = int(max(1, min(r, cap, max(1, rate * self.target_ms))))
+                b.sweep(r, measure=True)
+                m = b.mark()
+                in_flight.append((m, r))
+                for l in running:
+                    if left[l]:
+                        left[l] = max(0, left[l] - r)
+                        if left[l] == 0:
+                            finishing.setdefault(m, []).append(l)
                 continue
-            k = int(max(1, min(self.max_rounds, self.target_ms / max(round_ms, 1e-3))))
-            t_a = time.perf_counter()
-            self.batch.sweep(k, measure=True)
-            left, _ = self.batch.poll()
-            round_ms = 0.7 * round_ms + 0.3 * (time.perf_counter() - t_a) * 1e3 / k
-            finished = [lid for lid in running if left[lid] == 0]
-            for lid in finished:
-                job = running.pop(lid)
-                job.result = _result(self.batch.samples(lid), job.L, job.T, self.discard)
-                self.batch.remove(lid)
-                job.done = clock()
+            if in_flight:
+                m, r = in_flight[0]
+                t_dev = b.mark_done(m)
+                if t_dev is None:
+                    time.sleep(0.0002)
+                    continue
+                in_flight.popleft()
+                if t_dev > last_mark_time[0]:
+                    rate = 0.7 * rate + 0.3 * r / max((t_dev - last_mark_time[0]) * 1e3, 1e-3)
+                last_mark_time = (t_dev, r)
+                for l in finishing.pop(m, []):
+                    job = running.pop(l)
+                    left.pop(l)
+                    job.done = t_origin + t_dev
+                    n_samples = job.sweeps // self.measure_every if self.measure_every else 0
+                    job.result = _result(b.samples_finished(l, max(n_samples, 1)), job.L, job.T, self.discard)
+                    finished.append(l)
+                continue
+            if pending and not running:
+                time.sleep(max(0.0, min(pending[0].arrival - clock(), 0.005)))
+        release_finished()
         return jobs
 
 

@@ -180,7 +180,8 @@ int swb_attach_spins(swb_lattice *h, void *device_spins);
 int swb_device_alloc(int device, size_t bytes, void **ptr);
 int swb_device_free(int device, void *ptr);
 
-/* Synchronous host <-> device copies (hipMemcpy in ising/src/lattice.cpp:74,89). */
+/* Synchronous host <-> device copies (hipMemcpy in ising/src/lattice.cpp:74,89): each first
+ * waits for all work queued on the device (the handles' streams included). */
 int swb_copy_to_device(int device, void *dst, const void *src, size_t bytes);
 int swb_copy_to_host(int device, void *dst, const void *src, size_t bytes);
 
@@ -194,7 +195,9 @@ int swb_device_sm_count(int device, uint32_t *count);
 /* Energy and magnetisation per site of any device spin array (L0 x L1, 0/1), reduced on the
  * device: out[0] = E/N, out[1] = M/N, the integer sums to e_sum / m_sum (each may be NULL).
  * Lattice<2>::GetEnergyAndMagnetization<AMD_GPU> copies the spins to the host for this
- * (ising/src/lattice.cpp:70-79).  Synchronous; calls on one device are serialised. */
+ * (ising/src/lattice.cpp:70-79).  Synchronous: it first waits for all work queued on the device,
+ * so a lattice swept on a handle's stream is measured after those sweeps; calls on one device
+ * are serialised. */
 int swb_spins_energy_magnetization(int device, uint32_t L0, uint32_t L1, const void *device_spins, double *out,
                                    int64_t *e_sum, int64_t *m_sum);
 
@@ -211,8 +214,8 @@ int swb_update_host(swb_lattice *h, float temperature, const uint8_t *spins_in, 
  * current device: spins[L0*L1] (0/1, 16-byte aligned), rng_state[n_tiles*W], rng_sel[n_tiles*W]
  * (index 0..4 of the lcg32 parameter pair, random/src/lcg32.cpp:17-24), rng_iter[n_tiles],
  * n_tiles = ceil(L0/tile_x) * ceil(L1/tile_y) -- the layout swb_get_rng exports.  Results equal
- * swb_sweep's on the same state.  The label array, block edge words and fault word live in one
- * static device array of 24 MiB + 1 KiB, so L0*L1 is at most 4,194,304 (2048 x 2048); larger
+ * swb_sweep's on the same state.  The label array, block edge records and fault word live in one
+ * static device array of 26 MiB, so L0*L1 is at most 4,194,304 (2048 x 2048); larger
  * lattices return SWB_ERR_CAPACITY before any CUDA call.  All calls on a device share that array
  * (each call clears its fault word, the kernels overwrite the rest): calls that overlap on the
  * GPU race, so serialise them (one stream, or events).  The first call on each device looks the
@@ -284,6 +287,14 @@ int swb_batch_poll(swb_batch *b, uint32_t *sweeps_left, uint32_t *sweeps_done);
 /* n_rounds rounds: every lattice with sweeps left sweeps once per round.  measure != 0 adds
  * the measurement phase.  Asynchronous (CUDA graph replays on the batch's stream). */
 int swb_batch_sweep(swb_batch *b, uint32_t n_rounds, int measure);
+
+/* Non-blocking progress, for a host loop that keeps the device busy without waiting on it:
+ * swb_batch_mark records a point after the work submitted so far (ids count up from 0; the
+ * last 64 stay queryable), swb_batch_mark_query tells whether the device has passed it
+ * (*done) and, if so, its time in ms since the first mark (*ms, may be NULL), from device
+ * events.  No counterpart in the reference, whose GPU path synchronises after every kernel. */
+int swb_batch_mark(swb_batch *b, uint32_t *mark);
+int swb_batch_mark_query(swb_batch *b, uint32_t mark, int *done, double *ms);
 int swb_batch_synchronize(swb_batch *b);
 
 /* Like swb_batch_sweep without measurement, timed with CUDA events: ms[0] total; with
@@ -294,6 +305,13 @@ int swb_batch_sweep_timed(swb_batch *b, uint32_t n_rounds, int per_kernel, float
 /* Per-lattice observables, as swb_accumulators / swb_samples. */
 int swb_batch_accumulators(swb_batch *b, uint32_t id, double *out);
 int swb_batch_samples(swb_batch *b, uint32_t id, int64_t *em, uint64_t capacity, uint64_t *count);
+
+/* The same read for a lattice that has finished its sweep budget, without waiting for the
+ * batch's other work: valid once a mark (swb_batch_mark) recorded after the lattice's last sweep
+ * has been passed (no later round writes its samples); acc[4] (may be NULL) receives its
+ * accumulators as swb_batch_accumulators does. */
+int swb_batch_samples_finished(swb_batch *b, uint32_t id, int64_t *em, uint64_t capacity, uint64_t *count,
+                               double *acc);
 int swb_batch_get_rng(swb_batch *b, uint32_t id, uint32_t *state, uint32_t *a, uint32_t *c, uint32_t *iteration);
 /* Imports lattice id's lcg32 streams (as swb_set_rng): with the spins, the whole state a
  * preempted job needs to resume bit-identically.  Synchronous. */

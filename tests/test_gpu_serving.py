@@ -1,5 +1,6 @@
-"""Continuous batching: jobs that share the GPU give the same results as alone, the HBM budget
-gates admission, and every admitted job finishes at exactly its sweep count."""
+"""Continuous batching: jobs that share the GPU give the same results as alone and as the CPU
+restatement of the reference, the HBM budget gates admission, and every admitted job finishes at
+exactly its sweep count."""
 import numpy as np
 import pytest
 
@@ -25,6 +26,7 @@ def test_results_same_alone_and_in_mix(gpu):
         s = Server(hbm_budget_bytes=0, capacity=1)
         s.run([solo], realtime=False)
         s.close()
+        assert np.array_equal(solo.result.pop("series"), j.result.pop("series")), j
         assert solo.result == j.result, j
 
 
@@ -58,3 +60,25 @@ def test_realtime_poisson_latency(gpu):
     s = latency_summary(jobs)
     assert s["jobs"] == 24 and s["p99_s"] >= s["p50_s"] > 0
     assert all(np.isfinite(j.result["E"]) for j in jobs)
+
+
+def test_served_series_equal_the_oracle(gpu, oracle):
+    """Jobs served together: each job's recorded (e, m) integer series is the restatement's for
+    that job alone (hot start and lcg32 streams from the job's seed, the served tile)."""
+    from computational_physics_b200 import autotune
+    from oracle import num_tiles
+    jobs = [Job(0, 32, 2.1, 120, 7), Job(1, 48, 2.6, 200, 8), Job(2, 64, 2.27, 90, 9), Job(3, 96, 3.0, 150, 10)]
+    srv = Server(hbm_budget_bytes=0, capacity=8, measure_every=10)
+    srv.run(jobs, realtime=False)
+    srv.close()
+    table = autotune.load()
+    for j in jobs:
+        tile, _ = autotune.choice(j.L, table)
+        spins = oracle.hot_start(j.L, j.L, j.seed)
+        rng = oracle.rng_init(16, num_tiles(j.L, j.L, *tile), j.seed)
+        want = []
+        for k in range(j.sweeps):
+            oracle.sweep(spins, tile[0], tile[1], rng, T=j.T)
+            if (k + 1) % 10 == 0:
+                want.append(oracle.energy_magnetization(spins))
+        assert [tuple(x) for x in j.result["series"]] == want, j.jid

@@ -17,6 +17,7 @@ class FakeBatch:
 
     def __init__(self, capacity, budget, lcg_width=16, device=0):
         self.capacity, self.budget = capacity, budget
+        self.rounds = 0
         self.lat = {}
         self.max_used = 0
         self.max_running = 0
@@ -41,6 +42,7 @@ class FakeBatch:
         self.lat[lid].update(left=sweeps, every=measure_every)
 
     def sweep(self, rounds=1, measure=False):
+        self.rounds += rounds
         for v in self.lat.values():
             for _ in range(min(rounds, v["left"])):
                 v["left"] -= 1
@@ -59,6 +61,18 @@ class FakeBatch:
 
     def samples(self, lid):
         return np.array(self.lat[lid]["samples"], np.int64).reshape(-1, 2)
+
+    def samples_finished(self, lid, max_samples):
+        assert self.lat[lid]["left"] == 0, "read before the lattice finished"
+        return self.samples(lid)[:max_samples]
+
+    # device progress: the fake runs rounds at once; a mark's "device time" is 0.1 ms per round
+    def mark(self):
+        self.marks = getattr(self, "marks", []) + [self.rounds]
+        return len(self.marks) - 1
+
+    def mark_done(self, m):
+        return 1e-4 * self.marks[m]
 
     def remove(self, lid):
         del self.lat[lid]
@@ -98,6 +112,30 @@ def test_admission_respects_budget_and_every_job_completes(fake):
         assert abs(j.result["E"] - j.result["exact_E"]) < 1e-3
     admitted = [j.admitted for j in sorted(jobs, key=lambda j: j.arrival)]
     assert admitted == sorted(admitted)                            # first come, first admitted
+
+
+def test_bounded_bypass_of_a_head_job_that_does_not_fit(fake):
+    """A big job at the head waits for memory; small jobs behind it go ahead, but only
+    max_bypass of them, after which the head is served first."""
+    sides = [64, 64, 128] + [32] * 6
+    jobs = _jobs(sides, [400, 400, 100] + [50] * 6)
+    srv = serving.Server(hbm_budget_bytes=128 * 128, capacity=8, measure_every=10, max_bypass=2)
+    srv.run(jobs, realtime=False)
+    assert not srv.rejected and all(j.done is not None for j in jobs)
+    assert srv.bypassed == 2
+    big = jobs[2]
+    ahead = [j for j in jobs[3:] if j.admitted < big.admitted]
+    assert len(ahead) == 2
+
+
+def test_jobs_finish_in_their_own_round(fake):
+    """A job's completion is the device time of the mark after its last round: with jobs of
+    100, 200, 300 sweeps admitted together, 0.1 ms per round in the fake."""
+    jobs = _jobs([32, 32, 32], [100, 200, 300])
+    srv = serving.Server(hbm_budget_bytes=10 ** 9, capacity=4, measure_every=10, max_rounds=10 ** 6)
+    srv.run(jobs, realtime=False)
+    d = [j.done for j in jobs]
+    assert d[1] - d[0] == pytest.approx(100 * 1e-4, abs=1e-6) and d[2] - d[1] == pytest.approx(100 * 1e-4, abs=1e-6)
 
 
 def test_slot_limit_holds_back_jobs(fake):
