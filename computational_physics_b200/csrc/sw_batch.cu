@@ -27,7 +27,8 @@
 
 namespace swb {
 
-constexpr uint32_t kBatchThreads = 512;        // CTA size of the assign and measure kernels
+constexpr uint32_t kBatchThreads = 512;        // CTA size of the assign kernel
+constexpr uint32_t kMeasureThreads = 256;      // measure: one thread per 16 sites of a 4096-site chunk
 constexpr uint32_t kMergeThreads = 192;        // merge: one thread per block edge site (BX + BY <= 160)
 constexpr uint32_t kFlipThreads = 256;         // flip: four quads of a 128 x 32 block per thread
 constexpr uint32_t kChunkSites = 4096;         // measure work item
@@ -51,29 +52,15 @@ struct BatchLat {
     uint32_t swept;           // 1 if this lattice was swept in the current round
     uint32_t measure_every;   // measure after every measure_every-th sweep (0: never)
     uint32_t sweeps_done;     // sweeps completed
-    uint32_t pad;
+    uint32_t measure_base;    // first entry of this lattice's chunks in the round's measure list
 };
 
 struct BatchCounters {
-    unsigned int measure_next;  // next measure chunk (device work counter)
-    unsigned int n_active;      // lattices in the work lists
-    unsigned int total_chunks;  // measure chunks of all active lattices
-    unsigned int pad;
+    unsigned int measure_next;    // next entry of the measure list (device work counter)
+    unsigned int n_active;        // lattices in the work lists
+    unsigned int total_chunks;    // measure chunks of all active lattices (the list's capacity)
+    unsigned int measure_chunks;  // entries of this round's measure list
 };
-
-// Lattice of work item `item`: largest k with prefix[k] <= item.
-__device__ __forceinline__ uint32_t find_lattice(const uint32_t *prefix, uint32_t n, uint32_t item)
-{
-    uint32_t lo = 0, hi = n;  // prefix[lo] <= item < prefix[hi]
-    while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (prefix[mid] <= item)
-            lo = mid;
-        else
-            hi = mid;
-    }
-    return lo;
-}
 
 __device__ __forceinline__ uint32_t next_item(unsigned int *queue, uint32_t *slot)
 {
@@ -96,8 +83,6 @@ __global__ void __launch_bounds__(kBatchThreads, 4) kb_assign(BatchLat *lats, co
                                                               BatchCounters *ctr)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    if (blockIdx.x == 0 && threadIdx.x == 0)
-        ctr->measure_next = 0;  // measure of the previous round is finished
     uint2 d = load_item(items, blockIdx.x, total);
     for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
         const uint2 next = load_item(items, item + gridDim.x, total);
@@ -167,7 +152,10 @@ __global__ void __launch_bounds__(kFlipThreads, 6) kb_flip(BatchLat *lats, const
 // Closes a round after every phase kernel of it (before the measurement): each lattice that was
 // swept counts the sweep and spends one from its budget.  The kernels of the round read the
 // budget only to skip finished lattices, so it changes here, between rounds.
-__global__ void kb_end_round(BatchLat *lats, const uint32_t *active, const BatchCounters *ctr)
+// With chunk_lat (a round that measures), every lattice due for a sample (measure_every divides
+// its sweep count) appends its 4096-site chunks to the round's measure list, so kb_measure visits
+// only those.
+__global__ void kb_end_round(BatchLat *lats, const uint32_t *active, BatchCounters *ctr, uint32_t *chunk_lat)
 {
     const uint32_t n = ctr->n_active;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
@@ -177,40 +165,51 @@ __global__ void kb_end_round(BatchLat *lats, const uint32_t *active, const Batch
             L->sweeps_done += 1;
             if (L->sweeps_left != kUnlimited)
                 L->sweeps_left -= 1;
+            if (chunk_lat && L->measure_every && L->sweeps_done % L->measure_every == 0) {
+                const uint32_t nch = (uint32_t)(((size_t)L->g.L0 * L->g.L1 + kChunkSites - 1) / kChunkSites);
+                const uint32_t base = atomicAdd(&ctr->measure_chunks, nch);
+                L->measure_base = base;
+                for (uint32_t c = 0; c < nch; ++c)
+                    chunk_lat[base + c] = active[k];
+            }
         }
     }
 }
 
-// Energy / magnetisation of lattices that completed a multiple of measure_every sweeps in
-// this round; per-lattice int64 sums, the last chunk turns them into FP64 accumulators.
-__global__ void __launch_bounds__(kBatchThreads) kb_measure(BatchLat *lats, const uint32_t *active,
-                                                            const uint32_t *chunk_prefix, BatchCounters *ctr)
+// Energy / magnetisation of the lattices on this round's measure list (kb_end_round): CTAs pull
+// 4096-site chunks from a device counter; per lattice int64 sums, the last chunk turns them into
+// FP64 accumulators.  A round whose list is empty costs one read per CTA.
+__global__ void __launch_bounds__(kMeasureThreads) kb_measure(BatchLat *lats, const uint32_t *chunk_lat,
+                                                              BatchCounters *ctr)
 {
     __shared__ uint32_t slot;
-    __shared__ long long se[kBatchThreads / 32], sm[kBatchThreads / 32];
-    const uint32_t n = ctr->n_active, total = ctr->total_chunks;
+    __shared__ long long se[kMeasureThreads / 32], sm[kMeasureThreads / 32];
+    const uint32_t total = ctr->measure_chunks;
+    if (total == 0)
+        return;
     while (true) {
         const uint32_t item = next_item(&ctr->measure_next, &slot);
         if (item >= total)
             break;
-        const uint32_t k = find_lattice(chunk_prefix, n, item);
-        BatchLat *L = lats + active[k];
-        if (!L->swept || L->measure_every == 0 || (L->sweeps_done % L->measure_every) != 0)
-            continue;
+        BatchLat *L = lats + chunk_lat[item];
         const uint32_t L0 = L->g.L0, L1 = L->g.L1;
         const size_t nsites = (size_t)L0 * L1;
-        const size_t i0 = (size_t)(item - chunk_prefix[k]) * kChunkSites;
-        const size_t i1 = min(i0 + kChunkSites, nsites);
-        const uint8_t *s = L->spins;
-        long long e = 0, m = 0;
-        for (size_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
-            const uint32_t y = (uint32_t)(i / L0), x = (uint32_t)(i - (size_t)y * L0);
-            const int v = 2 * s[i] - 1;
-            const int r = 2 * s[(size_t)y * L0 + (x + 1 == L0 ? 0 : x + 1)] - 1;
-            const int d = 2 * s[(size_t)(y + 1 == L1 ? 0 : y + 1) * L0 + x] - 1;
-            e += v * (r + d);
-            m += v;
+        const uint32_t chunk = item - L->measure_base;
+        const uint32_t nchunks = (uint32_t)((nsites + kChunkSites - 1) / kChunkSites);
+        const size_t i0 = (size_t)chunk * kChunkSites, i1 = min(i0 + kChunkSites, nsites);
+        int ei = 0, mi = 0;
+        // 16-site pieces (row_em's unit), cut at row ends: 256 of the CTA's threads per chunk
+        for (size_t p = i0 + (size_t)threadIdx.x * 16; p < i1; p += (size_t)blockDim.x * 16) {
+            size_t q = p;
+            const size_t qe = min(p + 16, i1);
+            while (q < qe) {
+                const uint32_t y = (uint32_t)(q / L0), x = (uint32_t)(q - (size_t)y * L0);
+                const uint32_t cnt = (uint32_t)min((size_t)(L0 - x), qe - q);
+                row_em(L->spins, L0, L1, y, x, cnt, ei, mi);
+                q += cnt;
+            }
         }
+        long long e = ei, m = mi;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             e += __shfl_xor_sync(0xffffffffu, e, o);
@@ -227,32 +226,7 @@ __global__ void __launch_bounds__(kBatchThreads) kb_measure(BatchLat *lats, cons
                 be += se[w];
                 bm += sm[w];
             }
-            Obs *o = L->obs;
-            atomicAdd(&o->e, (unsigned long long)be);
-            atomicAdd(&o->m, (unsigned long long)bm);
-            __threadfence();
-            const uint32_t nchunks = chunk_prefix[k + 1] - chunk_prefix[k];
-            if (atomicAdd(&o->done, 1u) == nchunks - 1) {
-                __threadfence();
-                const long long te = (long long)atomicAdd(&o->e, 0ull);
-                const long long tm = (long long)atomicAdd(&o->m, 0ull);
-                o->last_e = te;
-                o->last_m = tm;
-                const double E = -(double)te / (double)nsites, M = (double)tm / (double)nsites;
-                o->acc[0] += E;
-                o->acc[1] += E * E;
-                o->acc[2] += fabs(M);
-                o->acc[3] += 1.0;
-                const unsigned long long j = o->n_samples;
-                if (j < L->series_cap) {
-                    L->series[2 * j] = te;
-                    L->series[2 * j + 1] = tm;
-                }
-                o->n_samples = j + 1;
-                o->e = 0;
-                o->m = 0;
-                o->done = 0;
-            }
+            obs_add_part(L->obs, L->series, L->series_cap, nsites, nchunks, be, bm, 1);
         }
         __syncthreads();
     }
@@ -261,6 +235,10 @@ __global__ void __launch_bounds__(kBatchThreads) kb_measure(BatchLat *lats, cons
 // Clears the per-round "swept" flags (first node of a round).
 __global__ void kb_begin_round(BatchLat *lats, const uint32_t *active, BatchCounters *ctr)
 {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {  // the previous round's measurement is finished
+        ctr->measure_next = 0;
+        ctr->measure_chunks = 0;
+    }
     const uint32_t n = ctr->n_active;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
         lats[active[k]].swept = 0;
@@ -268,28 +246,9 @@ __global__ void kb_begin_round(BatchLat *lats, const uint32_t *active, BatchCoun
 
 template <int W>
 __global__ void kb_rng_init(const uint32_t n_tiles, const uint32_t seed_base, uint32_t *state, uint8_t *sel,
-                            uint32_t *iter)
+                           uint32_t *iter)
 {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n_tiles)
-        return;
-    uint64_t x = drand48_seed(seed_base + t);
-    uint32_t s[W];
-#pragma unroll
-    for (int i = 0; i < W; ++i) {
-        x = drand48_step(x);
-        s[i] = ((uint32_t)__dmul_rn(1000.0, drand48_value(x))) % 5u;
-        sel[(size_t)t * W + i] = (uint8_t)s[i];
-    }
-    x = drand48_step(x);
-    uint32_t v = lcg_param_a(s[0]) * ((uint32_t)__dmul_rn(4026531839.0, drand48_value(x)) + 1u) + lcg_param_c(s[0]);
-    state[(size_t)t * W] = v;
-#pragma unroll
-    for (int i = 1; i < W; ++i) {
-        v = lcg_param_a(s[i]) * v + lcg_param_c(s[i]);
-        state[(size_t)t * W + i] = v;
-    }
-    iter[t] = 0;
+    rng_init_tile<W>(n_tiles, seed_base, state, sel, iter);
 }
 
 // One lattice's spins and its slice of the contiguous staging buffer (host transfers).
@@ -299,40 +258,36 @@ struct StageCopy {
     unsigned long long bytes;
 };
 
-// Staging buffer -> lattice spins (to_lattice != 0) or back, one CTA per lattice; 16-byte
-// moves when both ends and the length allow, else 4-byte or single-byte moves.
-__global__ void kb_stage_copy(const StageCopy *c, uint8_t *stage, const int to_lattice)
+// Staging buffer -> lattice spins (to_lattice != 0) or back: CTA (x, y) moves piece x (kStagePiece
+// bytes) of lattice y of the group; 16-byte moves when both ends and the length allow, else 4-byte
+// or single-byte moves.
+constexpr uint32_t kStagePiece = 16384;
+
+__global__ void __launch_bounds__(256) kb_stage_copy(const StageCopy *c, uint8_t *stage, const int to_lattice)
 {
-    const StageCopy d = c[blockIdx.x];
-    uint8_t *a = to_lattice ? d.spins : stage + d.offset;
-    const uint8_t *s = to_lattice ? stage + d.offset : d.spins;
-    const uintptr_t align = (uintptr_t)a | (uintptr_t)s | (uintptr_t)d.bytes;
+    const StageCopy d = c[blockIdx.y];
+    const size_t p0 = (size_t)blockIdx.x * kStagePiece;
+    if (p0 >= d.bytes)
+        return;
+    const size_t len = min((size_t)kStagePiece, (size_t)d.bytes - p0);
+    uint8_t *a = (to_lattice ? d.spins : stage + d.offset) + p0;
+    const uint8_t *s = (to_lattice ? stage + d.offset : d.spins) + p0;
+    const uintptr_t align = (uintptr_t)a | (uintptr_t)s | (uintptr_t)len;
     if ((align & 15u) == 0) {
-        for (size_t i = threadIdx.x; i < d.bytes / 16; i += blockDim.x)
+        for (size_t i = threadIdx.x; i < len / 16; i += blockDim.x)
             reinterpret_cast<uint4 *>(a)[i] = reinterpret_cast<const uint4 *>(s)[i];
     } else if ((align & 3u) == 0) {
-        for (size_t i = threadIdx.x; i < d.bytes / 4; i += blockDim.x)
+        for (size_t i = threadIdx.x; i < len / 4; i += blockDim.x)
             reinterpret_cast<uint32_t *>(a)[i] = reinterpret_cast<const uint32_t *>(s)[i];
     } else {
-        for (size_t i = threadIdx.x; i < d.bytes; i += blockDim.x)
+        for (size_t i = threadIdx.x; i < len; i += blockDim.x)
             a[i] = s[i];
     }
 }
 
 __global__ void kb_hot_start(const size_t n, const uint32_t seed, uint8_t *spins)
 {
-    constexpr uint32_t kChunk = 64;
-    const size_t first = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) * kChunk;
-    if (first >= n)
-        return;
-    uint64_t A, C;
-    drand48_jump(first, A, C);
-    uint64_t x = (A * drand48_seed(seed) + C) & kDrandMask;
-    const size_t last = first + kChunk < n ? first + kChunk : n;
-    for (size_t i = first; i < last; ++i) {
-        x = drand48_step(x);
-        spins[i] = (uint8_t)(x >> 47);
-    }
+    hot_start_chunk(n, seed, spins);
 }
 
 }  // namespace swb
@@ -357,7 +312,9 @@ struct swb_batch {
     uint64_t budget = 0, used = 0;
     std::vector<HostLat> lats;
     BatchLat *d_lats = nullptr;
-    uint32_t *d_active = nullptr, *d_chunk_prefix = nullptr;
+    uint32_t *d_active = nullptr;
+    uint32_t *d_chunk_lat = nullptr;      // the round's measure list: lattice slot per chunk
+    uint32_t chunk_lat_cap = 0;
     uint2 *d_items = nullptr;       // flat block list (lattice slot, byi << 16 | bxi)
     uint32_t items_cap = 0;
     uint32_t items_n = 0;           // block items in the list (the phase kernels' grid)
@@ -379,6 +336,7 @@ struct swb_batch {
         std::vector<uint32_t> ids, gs;
         std::vector<size_t> gi;
         std::vector<StageCopy> copies;
+        std::vector<uint64_t> max_bytes;  // largest lattice of each group (the stage copies' grid)
         uint64_t total = 0, version = ~0ull;
     } io;
     std::vector<cudaEvent_t> io_events;
@@ -419,7 +377,7 @@ uint64_t lattice_bytes(const Geo &g, uint32_t W, uint64_t series_cap)
 {
     const uint64_t n = (uint64_t)g.L0 * g.L1, tiles = (uint64_t)g.n0 * g.n1, blocks = (uint64_t)g.nbx * g.nby;
     auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
-    return al(n) + al(4 * n) + al(4 * tiles * W) + al(tiles * W) + al(4 * tiles) + al(4 * (uint64_t)edge_stride(g) * blocks) +
+    return al(n) + al(4 * n) + al(4 * tiles * W) + al(tiles * W) + al(4 * tiles) + al(4 * kEdgeWords * blocks) +
            al(4 * (uint64_t)(g.BX + g.BY) * blocks) + al(sizeof(Obs)) + al(16 * series_cap);
 }
 
@@ -490,6 +448,19 @@ int rebuild_lists(swb_batch *b)
         SWB_CUDA(cudaMalloc(&b->d_items, sizeof(uint2) * cap));
         b->items_cap = cap;
     }
+    if (cp[n] > b->chunk_lat_cap) {  // the measure list holds every active lattice's chunks
+        SWB_CUDA(cudaStreamSynchronize(b->stream));  // no captured round may still read the old list
+        for (auto &ge : b->graph)
+            if (ge) {
+                cudaGraphExecDestroy(ge);
+                ge = nullptr;
+            }
+        SWB_CUDA(cudaFree(b->d_chunk_lat));
+        b->d_chunk_lat = nullptr;
+        const uint32_t cap = std::max<uint32_t>(cp[n], 2 * b->chunk_lat_cap);
+        SWB_CUDA(cudaMalloc(&b->d_chunk_lat, sizeof(uint32_t) * cap));
+        b->chunk_lat_cap = cap;
+    }
     b->items_n = (uint32_t)items.size();
     BatchCounters c{};
     c.n_active = n;
@@ -498,7 +469,6 @@ int rebuild_lists(swb_batch *b)
         SWB_CUDA(cudaMemcpyAsync(b->d_items, items.data(), sizeof(uint2) * items.size(), cudaMemcpyHostToDevice,
                                  b->stream));
         SWB_CUDA(cudaMemcpyAsync(b->d_active, b->active.data(), n * 4, cudaMemcpyHostToDevice, b->stream));
-        SWB_CUDA(cudaMemcpyAsync(b->d_chunk_prefix, cp.data(), (n + 1) * 4, cudaMemcpyHostToDevice, b->stream));
     }
     SWB_CUDA(cudaMemcpyAsync(b->d_ctr, &c, sizeof(c), cudaMemcpyHostToDevice, b->stream));
     b->lists_dirty = false;
@@ -555,9 +525,9 @@ int launch_phases_b(swb_batch *b, const uint2 *items, uint32_t n, cudaStream_t s
     return launch_flip_b(b, items, n, st);
 }
 
-int launch_end_round(swb_batch *b, cudaStream_t st)
+int launch_end_round(swb_batch *b, cudaStream_t st, bool measure)
 {
-    kb_end_round<<<4, 128, 0, st>>>(b->d_lats, b->d_active, b->d_ctr);
+    kb_end_round<<<4, 128, 0, st>>>(b->d_lats, b->d_active, b->d_ctr, measure ? b->d_chunk_lat : nullptr);
     SWB_LAUNCHED();
     return SWB_OK;
 }
@@ -595,11 +565,10 @@ int launch_round(swb_batch *b, bool measure)
         SWB_CUDA(cudaEventRecord(b->join[q], b->gstream[q]));
         SWB_CUDA(cudaStreamWaitEvent(b->stream, b->join[q], 0));
     }
-    if (int rc = launch_end_round(b, b->stream))
+    if (int rc = launch_end_round(b, b->stream, measure))
         return rc;
     if (measure) {
-        kb_measure<<<b->grid_measure, kBatchThreads, 0, b->stream>>>(b->d_lats, b->d_active, b->d_chunk_prefix,
-                                                                   b->d_ctr);
+        kb_measure<<<b->grid_measure, kMeasureThreads, 0, b->stream>>>(b->d_lats, b->d_chunk_lat, b->d_ctr);
         SWB_LAUNCHED();
     }
     return SWB_OK;
@@ -702,12 +671,10 @@ int swb_batch_create(swb_batch **out, uint32_t capacity, uint64_t hbm_budget_byt
     SWB_TRY(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     SWB_TRY(cudaMalloc(&b->d_lats, sizeof(BatchLat) * capacity));
     SWB_TRY(cudaMalloc(&b->d_active, 4 * capacity));
-    SWB_TRY(cudaMalloc(&b->d_chunk_prefix, 4 * (capacity + 1)));
     SWB_TRY(cudaMalloc(&b->d_ctr, sizeof(BatchCounters)));
     SWB_TRY(cudaMalloc(&b->d_fault, sizeof(unsigned int)));
     SWB_TRY(cudaMemsetAsync(b->d_fault, 0, sizeof(unsigned int), b->stream));
     SWB_TRY(cudaMemsetAsync(b->d_ctr, 0, sizeof(BatchCounters), b->stream));
-    SWB_TRY(cudaMemsetAsync(b->d_chunk_prefix, 0, 4 * (capacity + 1), b->stream));
     // The assign phase may hold any block up to 128 x 32 sites: size shared memory for it.
     Geo gmax{};
     gmax.BX = 128; gmax.BY = 32;
@@ -715,7 +682,7 @@ int swb_batch_create(swb_batch **out, uint32_t capacity, uint64_t hbm_budget_byt
     b->smem_flip = flip_smem_bytes(gmax);
     int sms = 148, per_sm = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kb_measure, kBatchThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kb_measure, kMeasureThreads, 0);
     b->grid_measure = sms * std::max(per_sm, 1);  // measure: persistent, pulls chunks
     SWB_TRY(cudaStreamSynchronize(b->stream));
 #undef SWB_TRY
@@ -738,7 +705,7 @@ int swb_batch_destroy(swb_batch *b)
             cudaFree(l.mem);
     cudaFree(b->d_lats);
     cudaFree(b->d_active);
-    cudaFree(b->d_chunk_prefix);
+    cudaFree(b->d_chunk_lat);
     cudaFree(b->d_items);
     cudaFree(b->d_stage);
     cudaFree(b->d_copies);
@@ -814,7 +781,7 @@ int swb_batch_add(swb_batch *b, uint32_t L0, uint32_t L1, uint32_t tile_x, uint3
     d.rng_state = reinterpret_cast<uint32_t *>(p); p += al(4 * tiles * b->W);
     d.rng_sel = reinterpret_cast<uint8_t *>(p); p += al(tiles * b->W);
     d.rng_iter = reinterpret_cast<uint32_t *>(p); p += al(4 * tiles);
-    d.edge = reinterpret_cast<uint32_t *>(p); p += al(4 * (uint64_t)edge_stride(g) * blocks);
+    d.edge = reinterpret_cast<uint32_t *>(p); p += al(4 * kEdgeWords * blocks);
     d.linked = reinterpret_cast<uint32_t *>(p); p += al(4 * (uint64_t)(g.BX + g.BY) * blocks);
     d.obs = reinterpret_cast<Obs *>(p); p += al(sizeof(Obs));
     d.series = reinterpret_cast<long long *>(p);
@@ -1059,7 +1026,7 @@ int swb_batch_sweep_timed(swb_batch *b, uint32_t n_rounds, int per_kernel, float
             if ((rc = launch_flip_b(b, b->d_items, b->items_n, b->stream)))
                 break;
             SWB_CUDA(cudaEventRecord(ev[4], b->stream));
-            if ((rc = launch_end_round(b, b->stream)))
+            if ((rc = launch_end_round(b, b->stream, false)))
                 break;
             SWB_CUDA(cudaEventSynchronize(ev[4]));
             float t;
@@ -1304,6 +1271,10 @@ int swb_batch_update_host(swb_batch *b, uint32_t count, const uint32_t *ids, con
         P.gi = std::move(gi);
         P.copies = std::move(copies);
         P.total = total;
+        P.max_bytes.assign(P.gs.size() - 1, 0);
+        for (size_t q = 0; q + 1 < P.gs.size(); ++q)
+            for (uint32_t k = P.gs[q]; k < P.gs[q + 1]; ++k)
+                P.max_bytes[q] = std::max<uint64_t>(P.max_bytes[q], P.copies[k].bytes);
         P.version = b->lists_version;
     }
     const uint32_t G = (uint32_t)P.gs.size() - 1;
@@ -1341,14 +1312,15 @@ int swb_batch_update_host(swb_batch *b, uint32_t count, const uint32_t *ids, con
         for (uint32_t g = 0; g < G; ++g) {
             const uint32_t n = gs[g + 1] - gs[g];
             SWB_CUDA(cudaStreamWaitEvent(b->stream, ev[g], 0));
-            kb_stage_copy<<<n, 512, 0, b->stream>>>(b->d_copies + gs[g], b->d_stage, 1);
+            const dim3 sgrid((uint32_t)((P.max_bytes[g] + kStagePiece - 1) / kStagePiece), n);
+            kb_stage_copy<<<sgrid, 256, 0, b->stream>>>(b->d_copies + gs[g], b->d_stage, 1);
             SWB_LAUNCHED();
             if (int rc = launch_phases_b(b, b->d_io_items + gi[g + 1], (uint32_t)(gi[g + 2] - gi[g + 1]), b->stream))
                 return rc;
-            kb_stage_copy<<<n, 512, 0, b->stream>>>(b->d_copies + gs[g], b->d_stage, 0);
+            kb_stage_copy<<<sgrid, 256, 0, b->stream>>>(b->d_copies + gs[g], b->d_stage, 0);
             SWB_LAUNCHED();
             if (g + 1 == G)  // every listed and unlisted lattice has swept: close the round
-                if (int rc = launch_end_round(b, b->stream))
+                if (int rc = launch_end_round(b, b->stream, false))
                     return rc;
             SWB_CUDA(cudaEventRecord(ev[G + g], b->stream));
             SWB_CUDA(cudaStreamWaitEvent(b->s_out, ev[G + g], 0));

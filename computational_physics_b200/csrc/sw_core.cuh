@@ -23,10 +23,9 @@ extern std::atomic<uint64_t> g_launches;
 int fail(int code, const char *fmt, ...);
 
 // swb_sweep_static's scratch: one file-scope device array (sw_static_scratch.cu) holding the
-// label array, the block edge records and the fault word of a lattice of at most 2048 x 2048
-// sites: 16 MiB of labels plus at most 2.2 bytes per site of edge records (tile 8 x 2).
+// label array, the block edge words and the fault word of a lattice of at most 2048 x 2048 sites.
 constexpr uint64_t kStaticMaxSites = 1ull << 22;               // 2048 x 2048 sites
-constexpr size_t kStaticScratchBytes = 26ull << 20;            // 26 MiB
+constexpr size_t kStaticScratchBytes = (24ull << 20) + 1024;   // labels 16 MiB + edge words + fault
 // Device address of that array on `device`, which must be current (looked up once per device).
 int static_scratch_base(int device, unsigned char **base);
 
@@ -137,6 +136,67 @@ struct Obs {
     unsigned long long n_samples;  // samples recorded (may exceed capacity)
 };
 
+// LCG32_State<W>::Init (random/src/lcg32.cpp:27-49) of tile t = this thread, seeded seed_base + t:
+// drand48 draws pick each lane's (a, c) pair and the first lane's start, the others follow from
+// it.  The two double multiplications are rounded as the host's (__dmul_rn).
+template <int W>
+__device__ __forceinline__ void rng_init_tile(const uint32_t n_tiles, const uint32_t seed_base, uint32_t *state,
+                                              uint8_t *sel, uint32_t *iter)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_tiles)
+        return;
+    uint64_t x = drand48_seed(seed_base + t);
+    uint32_t s[W];
+#pragma unroll
+    for (int i = 0; i < W; ++i) {
+        x = drand48_step(x);
+        s[i] = ((uint32_t)__dmul_rn(1000.0, drand48_value(x))) % 5u;
+        sel[(size_t)t * W + i] = (uint8_t)s[i];
+    }
+    x = drand48_step(x);
+    uint32_t v = lcg_param_a(s[0]) * ((uint32_t)__dmul_rn(4026531839.0, drand48_value(x)) + 1u) + lcg_param_c(s[0]);
+    state[(size_t)t * W] = v;
+#pragma unroll
+    for (int i = 1; i < W; ++i) {
+        v = lcg_param_a(s[i]) * v + lcg_param_c(s[i]);
+        state[(size_t)t * W + i] = v;
+    }
+    iter[t] = 0;
+}
+
+// Hot start of Lattice<2> (ising/src/lattice.cpp:15-27), one 64-site chunk per thread: site i
+// takes drand48 draw i + 1 after srand48(seed); drand48() < 0.5 iff bit 47 of the 48-bit state is
+// clear.  The chunk's first state comes by jump-ahead; whole chunks store 8 sites at a time.
+__device__ __forceinline__ void hot_start_chunk(const size_t n, const uint32_t seed, uint8_t *spins)
+{
+    constexpr uint32_t kChunk = 64;
+    const size_t first = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) * kChunk;
+    if (first >= n)
+        return;
+    uint64_t A, C;
+    drand48_jump(first, A, C);
+    uint64_t x = (A * drand48_seed(seed) + C) & kDrandMask;
+    const size_t last = first + kChunk < n ? first + kChunk : n;
+    if (last - first == kChunk && (reinterpret_cast<uintptr_t>(spins) & 7u) == 0) {
+#pragma unroll
+        for (uint32_t q = 0; q < kChunk / 8; ++q) {
+            uint64_t v = 0;
+#pragma unroll
+            for (uint32_t k = 0; k < 8; ++k) {
+                x = drand48_step(x);
+                v |= (x >> 47) << (8 * k);
+            }
+            reinterpret_cast<uint64_t *>(spins + first)[q] = v;
+        }
+        return;
+    }
+    for (size_t i = first; i < last; ++i) {
+        x = drand48_step(x);
+        spins[i] = (uint8_t)(x >> 47);
+    }
+}
+
 // One part of a measurement: adds this part's integer sums (e = sum s (s_right + s_down),
 // m = sum s over its sites) and, if it is the last of n_parts, turns the totals into E/N and
 // M/N, accumulates E, E^2, |M| in FP64 (with accumulate), appends (e, m) to the series and
@@ -193,40 +253,6 @@ struct AssignDump {
     uint32_t *block_labels;
     uint32_t *tile_labels;
 };
-
-// The per-block edge record: kEdgeWords bond words ([0] the right edge's bonds by row, [1..4]
-// the bottom edge's by column), then the global root index of every site on the block's four
-// edges, written by the assign phase so that the merge reads them coalesced instead of
-// gathering label columns: right column [BY], left column [BY], bottom row [BX], top row [BX].
-__host__ __device__ inline uint32_t edge_stride(const Geo &g) { return kEdgeWords + 2 * (g.BX + g.BY); }
-
-// Fills the root part of block (bxi, byi)'s edge record, one slot per thread: root(l) gives the
-// block-local index of the root of block-local site l (its component's minimum).
-template <class Root>
-__device__ __forceinline__ void edge_roots(const Geo &g, const uint32_t bxi, const uint32_t byi, uint32_t *__restrict__ er,
-                                           const Root &root)
-{
-    const uint32_t BX = g.BX, BY = g.BY, x0 = bxi * BX, y0 = byi * BY;
-    const uint32_t bxv = min(BX, g.L0 - x0), byv = min(BY, g.L1 - y0);
-    for (uint32_t i = threadIdx.x; i < 2 * (BX + BY); i += blockDim.x) {
-        uint32_t xl, yl;
-        if (i < 2 * BY) {  // right column, then left column
-            yl = i < BY ? i : i - BY;
-            xl = i < BY ? bxv - 1 : 0;
-            if (yl >= byv)
-                continue;
-        } else {           // bottom row, then top row
-            const uint32_t j = i - 2 * BY;
-            xl = j < BX ? j : j - BX;
-            yl = j < BX ? byv - 1 : 0;
-            if (xl >= bxv)
-                continue;
-        }
-        const uint32_t r = root(yl * BX + xl);
-        const uint32_t ry = (BX & (BX - 1)) == 0 ? r >> (__ffs(BX) - 1) : r / BX;  // BX: a power of two but
-        er[kEdgeWords + i] = (y0 + ry) * g.L0 + x0 + (r - ry * BX);               // where the caller chose it
-    }
-}
 
 struct AssignSmem {
     uint32_t parent, draws, slots, edge, bond, sp, plab, total, pitch;
@@ -311,6 +337,31 @@ __device__ __forceinline__ uint32_t spin_bits32(const uint8_t *p)
     const uint4 a = *reinterpret_cast<const uint4 *>(p), b = *reinterpret_cast<const uint4 *>(p + 16);
     return spin_nibble(a.x) | spin_nibble(a.y) << 4 | spin_nibble(a.z) << 8 | spin_nibble(a.w) << 12 |
            spin_nibble(b.x) << 16 | spin_nibble(b.y) << 20 | spin_nibble(b.z) << 24 | spin_nibble(b.w) << 28;
+}
+
+// Energy / magnetisation sums of the `cnt` sites x0 .. x0 + cnt - 1 of row y of an L0 x L1
+// periodic lattice: e = sum s (s_right + s_down), m = sum s, s = 2 b - 1.  Rows 16-byte aligned
+// (L0 % 16 == 0) and 16-site aligned pieces go 16 sites at a time through bit masks (two 16-byte
+// loads, the byte after them, popcounts); anything else site by site.  No per-site division.
+__device__ __forceinline__ void row_em(const uint8_t *__restrict__ spins, const uint32_t L0, const uint32_t L1,
+                                       const uint32_t y, uint32_t x0, uint32_t cnt, int &e, int &m)
+{
+    const uint8_t *row = spins + (size_t)y * L0, *down = spins + (size_t)(y + 1 == L1 ? 0 : y + 1) * L0;
+    if ((L0 & 15u) == 0) {
+        for (; cnt >= 16 && (x0 & 15u) == 0; x0 += 16, cnt -= 16) {
+            const uint4 a = *reinterpret_cast<const uint4 *>(row + x0), d = *reinterpret_cast<const uint4 *>(down + x0);
+            const uint32_t S = spin_nibble(a.x) | spin_nibble(a.y) << 4 | spin_nibble(a.z) << 8 | spin_nibble(a.w) << 12;
+            const uint32_t D = spin_nibble(d.x) | spin_nibble(d.y) << 4 | spin_nibble(d.z) << 8 | spin_nibble(d.w) << 12;
+            const uint32_t R = (S >> 1) | ((uint32_t)row[x0 + 16 == L0 ? 0 : x0 + 16] << 15);
+            e += 32 - 2 * (__popc(S ^ R) + __popc(S ^ D));
+            m += 2 * __popc(S) - 16;
+        }
+    }
+    for (; cnt; ++x0, --cnt) {
+        const int v = 2 * row[x0] - 1;
+        e += v * ((2 * row[x0 + 1 == L0 ? 0 : x0 + 1] - 1) + (2 * down[x0] - 1));
+        m += v;
+    }
 }
 
 // Labelling of a block whose width is a multiple of 32, from the staged spins (sp) and the
@@ -429,7 +480,10 @@ __device__ __forceinline__ void dump_block(const Geo &g, const uint32_t bxi, con
     }
 }
 
-template <int W, int TXc, int TYc, bool kMayDump>
+// kBX, kBY, kThreads: the block shape and CTA size as compile-time constants (the common full
+// 128 x 32 block of 512 threads: the scanline then runs one band per warp with its rows
+// unrolled), or 0 for the runtime shape.
+template <int W, int TXc, int TYc, bool kMayDump, int kBX = 0, int kBY = 0, int kThreads = 0>
 __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uint32_t bxi, const uint32_t byi,
                                                          uint32_t *__restrict__ labels, uint32_t *__restrict__ edge,
                                                          const AssignDump &dump, const MeasureArgs &meas,
@@ -438,10 +492,12 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
     const AssignSmem L = assign_smem(g, W);
     uint32_t *parent = reinterpret_cast<uint32_t *>(smem + L.parent);
     uint32_t *edge_s = reinterpret_cast<uint32_t *>(smem + L.edge);
-    const uint32_t BX = g.BX, BY = g.BY, NW = BX >> 5, lnw = __ffs(NW) - 1;  // NW is a power of two
+    const uint32_t BX = kBX ? kBX : g.BX, BY = kBY ? kBY : g.BY;
+    const uint32_t NW = BX >> 5, lnw = __ffs(NW) - 1;             // NW is a power of two
     uint32_t *Xw = reinterpret_cast<uint32_t *>(smem + L.bond);  // [BY][NW] x-bonds inside the block
     uint32_t *Yw = Xw + BY * NW;                                  // [BY][NW] y-bonds inside the block
-    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t nwarps = kThreads ? kThreads / 32 : blockDim.x >> 5;
     const uint32_t x0 = bxi * BX, y0 = byi * BY;
     const uint32_t bxv = min(BX, g.L0 - x0), byv = min(BY, g.L1 - y0);
 
@@ -466,31 +522,53 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
     const uint32_t rb = (nb & (nb - 1)) == 0 ? (BY + nb - 1) >> (__ffs(nb) - 1)  // rows per band
                                              : (BY + nb - 1) / nb;
     const uint32_t below = (1u << lane) - 1u;                // lanes below this one
-    for (uint32_t task = warp; task < NW * nb; task += nwarps) {
-        const uint32_t sx = task & (NW - 1), band = task >> lnw;
-        const uint32_t ya = band * rb, yb = min(BY, ya + rb);
-        const uint32_t *xp = Xw + ya * NW + sx;  // this row's x-bond word; xp[BY * NW] its y-bond word
-        uint32_t base = ya * BX + (sx << 5);
-        uint32_t above = 0, Yup = 0, Xa = 0;     // the band's first row has no bonds up
-        for (uint32_t n = yb > ya ? yb - ya : 0; n != 0; --n) {
-            const uint32_t X = xp[0];
-            const uint32_t rs = 32 - __clz(~X & below);  // run start (lane); __clz(0) = 32
-            // The first y-bond or run end from the run start (bit 31 always ends a strip run):
-            // a y-bond there means the run inherits the label above it.
-            const uint32_t pos = __ffs((Yup | ~X | 0x80000000u) & (0xFFFFFFFFu << rs)) - 1;
-            const uint32_t rep = __shfl_sync(0xffffffffu, above, pos);
-            const uint32_t lab = ((Yup >> pos) & 1u) ? rep : base + rs;
-            // A y-bond whose left neighbour is bonded up too, with both rows bonded across, meets
-            // the same two runs as that neighbour's: only the leftmost of such a chain unites.
-            const uint32_t U = Yup & ~((Yup & X & Xa) << 1);
-            if (((U >> lane) & 1u) && above != lab)
-                uf_union(parent, above, lab);
-            plab[base + lane] = (uint16_t)lab;
-            above = lab;
+    // One row of a band: `above` holds the provisional label of the site above, Yup the row
+    // above's y-bond word, Xa its x-bond word.
+    auto row = [&](const uint32_t X, const uint32_t base, uint32_t &above, const uint32_t Yup, const uint32_t Xa) {
+        const uint32_t rs = 32 - __clz(~X & below);  // run start (lane); __clz(0) = 32
+        // The first y-bond or run end from the run start (bit 31 always ends a strip run):
+        // a y-bond there means the run inherits the label above it.
+        const uint32_t pos = __ffs((Yup | ~X | 0x80000000u) & (0xFFFFFFFFu << rs)) - 1;
+        const uint32_t rep = __shfl_sync(0xffffffffu, above, pos);
+        const uint32_t lab = ((Yup >> pos) & 1u) ? rep : base + rs;
+        // A y-bond whose left neighbour is bonded up too, with both rows bonded across, meets
+        // the same two runs as that neighbour's: only the leftmost of such a chain unites.
+        const uint32_t U = Yup & ~((Yup & X & Xa) << 1);
+        if (((U >> lane) & 1u) && above != lab)
+            uf_union(parent, above, lab);
+        plab[base + lane] = (uint16_t)lab;
+        above = lab;
+    };
+    if constexpr (kBX != 0) {
+        // one band per warp, its rows unrolled with compile-time offsets
+        static_assert(kBX == 128 && kBY == 32 && kThreads == 512, "the fixed shape is one band per warp");
+        constexpr uint32_t kNW = kBX / 32, kRows = kBY / ((kThreads / 32) / kNW);
+        const uint32_t sx = warp & (kNW - 1), ya = (warp / kNW) * kRows;
+        const uint32_t *xp = Xw + ya * kNW + sx;
+        const uint32_t base = ya * kBX + (sx << 5);
+        uint32_t above = 0, Yup = 0, Xa = 0;
+#pragma unroll
+        for (uint32_t r = 0; r < kRows; ++r) {
+            const uint32_t X = xp[r * kNW];
+            row(X, base + r * kBX, above, Yup, Xa);
             Xa = X;
-            Yup = xp[BY * NW];
-            xp += NW;
-            base += BX;
+            Yup = xp[kBY * kNW + r * kNW];
+        }
+    } else {
+        for (uint32_t task = warp; task < NW * nb; task += nwarps) {
+            const uint32_t sx = task & (NW - 1), band = task >> lnw;
+            const uint32_t ya = band * rb, yb = min(BY, ya + rb);
+            const uint32_t *xp = Xw + ya * NW + sx;  // this row's x-bond word; xp[BY * NW] its y-bond word
+            uint32_t base = ya * BX + (sx << 5);
+            uint32_t above = 0, Yup = 0, Xa = 0;     // the band's first row has no bonds up
+            for (uint32_t n = yb > ya ? yb - ya : 0; n != 0; --n) {
+                const uint32_t X = xp[0];
+                row(X, base, above, Yup, Xa);
+                Xa = X;
+                Yup = xp[BY * NW];
+                xp += NW;
+                base += BX;
+            }
         }
     }
     __syncthreads();
@@ -558,10 +636,8 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
             }
         }
     }
-    uint32_t *erec = edge + ((size_t)byi * g.nbx + bxi) * edge_stride(g);  // this block's edge record
-    edge_roots(g, bxi, byi, erec, [&](uint32_t l) { return uf_find_halve(parent, plab[l]); });
     if (tid < kEdgeWords)
-        erec[tid] = edge_s[tid];
+        edge[((size_t)byi * g.nbx + bxi) * kEdgeWords + tid] = edge_s[tid];
     if (meas.obs && tid == 0)  // the block's sums (complete since the barrier after the bond words)
         obs_add_part(meas.obs, meas.series, meas.cap, (size_t)g.L0 * g.L1, g.nbx * g.nby,
                      reinterpret_cast<const int *>(edge_s)[kEdgeE], reinterpret_cast<const int *>(edge_s)[kEdgeM], 1);
@@ -576,7 +652,7 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
 // kPhaseSeq selects the phase-dispatched draw sequence (below) for full-height tiles of a
 // compile-time shape: on B200 it is the faster form inside the batched kernel (whose item loop
 // keeps more registers live) and the slower one in the single-lattice kernel.
-template <int W, int TXc = 0, int TYc = 0, bool kPhaseSeq = false, bool kMayDump = true>
+template <int W, int TXc = 0, int TYc = 0, bool kPhaseSeq = false, bool kMayDump = true, bool kFixedShape = false>
 __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, const uint32_t byi,
                                              const uint8_t *__restrict__ spins, uint32_t *__restrict__ labels,
                                              uint32_t *__restrict__ rng_state, uint8_t *__restrict__ rng_sel,
@@ -796,6 +872,13 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
     __syncthreads();
 
     if (dump.tile_labels == nullptr && (BX & 31u) == 0 && (BX & (BX - 1)) == 0) {
+        if constexpr (kFixedShape && TXc != 0) {
+            if (BX == 128 && BY == 32 && nthr == 512) {
+                assign_block_labels_rows<W, TXc, TYc, kMayDump, 128, 32, 512>(g, bxi, byi, labels, edge, dump, meas,
+                                                                               smem);
+                return;
+            }
+        }
         assign_block_labels_rows<W, TXc, TYc, kMayDump>(g, bxi, byi, labels, edge, dump, meas, smem);
         return;
     }
@@ -887,10 +970,8 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
                 dump.block_labels[(size_t)(y0 + yl) * g.L0 + x0 + xl] = (y0 + r / BX) * g.L0 + x0 + r % BX;
         }
     }
-    edge_roots(g, bxi, byi, edge + ((size_t)byi * g.nbx + bxi) * edge_stride(g),
-               [&](uint32_t l) { return uf_find(parent, l); });
     if (tid < kEdgeWords)
-        edge[((size_t)byi * g.nbx + bxi) * edge_stride(g) + tid] = edge_s[tid];
+        edge[((size_t)byi * g.nbx + bxi) * kEdgeWords + tid] = edge_s[tid];
 }
 
 // assign_block with the tile shape as compile-time constants for the common shapes (lcg width
@@ -932,30 +1013,33 @@ __device__ __forceinline__ void merge_block(const Geo &g, const uint32_t bxi, co
 {
     const uint32_t x0 = bxi * g.BX, y0 = byi * g.BY;
     const uint32_t bxv = min(g.BX, g.L0 - x0), byv = min(g.BY, g.L1 - y0);
-    const uint32_t es = edge_stride(g);
-    const uint32_t *e = edge + ((size_t)byi * g.nbx + bxi) * es;
-    uint32_t a = 0, b = 0;
+    const uint32_t *e = edge + ((size_t)byi * g.nbx + bxi) * kEdgeWords;
+    size_t s = 0, nb = 0;
+    uint32_t nbx = bxi, nby = byi;  // block of the neighbour site
     bool go = false;
     if (t < g.BY) {
-        if (t < byv && ((e[0] >> t) & 1u)) {  // this block's right column, the next block's left column
-            const uint32_t nbx = bxi + 1 == g.nbx ? 0 : bxi + 1;
-            a = e[kEdgeWords + t];
-            b = edge[((size_t)byi * g.nbx + nbx) * es + kEdgeWords + g.BY + t];
+        if (t < byv && ((e[0] >> t) & 1u)) {
+            s = (size_t)(y0 + t) * g.L0 + x0 + bxv - 1;
+            nb = (size_t)(y0 + t) * g.L0 + (x0 + bxv < g.L0 ? x0 + bxv : 0u);
+            nbx = bxi + 1 == g.nbx ? 0 : bxi + 1;
             go = true;
         }
     } else {
         const uint32_t xl = t - g.BY;
-        if (xl < bxv && ((e[1 + (xl >> 5)] >> (xl & 31)) & 1u)) {  // this block's bottom row, the top row below
-            const uint32_t nby = byi + 1 == g.nby ? 0 : byi + 1;
-            a = e[kEdgeWords + 2 * g.BY + xl];
-            b = edge[((size_t)nby * g.nbx + bxi) * es + kEdgeWords + 2 * g.BY + g.BX + xl];
+        if (xl < bxv && ((e[1 + (xl >> 5)] >> (xl & 31)) & 1u)) {
+            s = (size_t)(y0 + byv - 1) * g.L0 + x0 + xl;
+            nb = (size_t)(y0 + byv < g.L1 ? y0 + byv : 0u) * g.L0 + x0 + xl;
+            nby = byi + 1 == g.nby ? 0 : byi + 1;
             go = true;
         }
     }
-    (void)x0; (void)y0;
     uint32_t link = kNoLink;
-    if (go && a != b)
-        link = guf_union_pair(labels, a, b, fault);
+    if (go) {
+        const volatile uint32_t *vl = labels;
+        const uint32_t a = label_global(g, bxi, byi, vl[s]), b = label_global(g, nbx, nby, vl[nb]);
+        if (a != b)
+            link = guf_union_pair(labels, a, b, fault);
+    }
     if (linked)
         linked[((size_t)byi * g.nbx + bxi) * (g.BX + g.BY) + t] = link;
 }

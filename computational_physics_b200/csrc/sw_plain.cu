@@ -82,8 +82,8 @@ __global__ void __launch_bounds__(kAssignThreads, 4) k_assign(const Geo g, const
                                                  const MeasureArgs meas)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    assign_block<W, TXc, TYc>(g, blockIdx.x, blockIdx.y, spins, labels, rng_state, rng_sel, rng_iter, thr, edge, dump,
-                              kMeasure ? meas : MeasureArgs{}, smem);
+    assign_block<W, TXc, TYc, false, true, true>(g, blockIdx.x, blockIdx.y, spins, labels, rng_state, rng_sel,
+                                                 rng_iter, thr, edge, dump, kMeasure ? meas : MeasureArgs{}, smem);
 }
 
 __global__ void __launch_bounds__(256) k_merge(const Geo g, const uint32_t *__restrict__ edge, uint32_t *labels,
@@ -121,17 +121,16 @@ __global__ void __launch_bounds__(256) k_measure(const uint32_t L0, const uint32
                                                  Obs *obs, long long *series, const unsigned long long cap,
                                                  const int accumulate)
 {
-    long long e = 0, m = 0;
+    // work items: 64-site pieces of rows (row_em takes them 16 sites at a time); a thread's
+    // partial sums stay far inside int range (at most 3 per site it visits)
     const size_t n = (size_t)L0 * L1;
-    const size_t stride = (size_t)gridDim.x * blockDim.x;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const uint32_t y = (uint32_t)(i / L0), x = (uint32_t)(i - (size_t)y * L0);
-        const int s = 2 * spins[i] - 1;
-        const int r = 2 * spins[(size_t)y * L0 + (x + 1 == L0 ? 0 : x + 1)] - 1;
-        const int d = 2 * spins[(size_t)(y + 1 == L1 ? 0 : y + 1) * L0 + x] - 1;
-        e += s * (r + d);
-        m += s;
+    const uint32_t per_row = (L0 + 63) / 64, items = per_row * L1;
+    int ei = 0, mi = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < items; i += gridDim.x * blockDim.x) {
+        const uint32_t y = i / per_row, x0 = (i - y * per_row) * 64;
+        row_em(spins, L0, L1, y, x0, min(64u, L0 - x0), ei, mi);
     }
+    long long e = ei, m = mi;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         e += __shfl_xor_sync(0xffffffffu, e, o);
@@ -159,44 +158,14 @@ template <int W>
 __global__ void k_rng_init(const uint32_t n_tiles, const uint32_t seed_base, uint32_t *state, uint8_t *sel,
                            uint32_t *iter)
 {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n_tiles)
-        return;
-    uint64_t x = drand48_seed(seed_base + t);
-    uint32_t s[W];
-#pragma unroll
-    for (int i = 0; i < W; ++i) {
-        x = drand48_step(x);
-        s[i] = ((uint32_t)__dmul_rn(1000.0, drand48_value(x))) % 5u;
-        sel[(size_t)t * W + i] = (uint8_t)s[i];
-    }
-    x = drand48_step(x);
-    uint32_t v = lcg_param_a(s[0]) * ((uint32_t)__dmul_rn(4026531839.0, drand48_value(x)) + 1u) + lcg_param_c(s[0]);
-    state[(size_t)t * W] = v;
-#pragma unroll
-    for (int i = 1; i < W; ++i) {
-        v = lcg_param_a(s[i]) * v + lcg_param_c(s[i]);
-        state[(size_t)t * W + i] = v;
-    }
-    iter[t] = 0;
+    rng_init_tile<W>(n_tiles, seed_base, state, sel, iter);
 }
 
 // Hot start of Lattice<2> (ising/src/lattice.cpp:24-26): site i takes drand48 draw i + 1
 // after srand48(seed); drand48() < 0.5 iff bit 47 of the 48-bit state is clear.
 __global__ void k_hot_start(const size_t n, const uint32_t seed, uint8_t *spins)
 {
-    constexpr uint32_t kChunk = 64;
-    const size_t first = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) * kChunk;
-    if (first >= n)
-        return;
-    uint64_t A, C;
-    drand48_jump(first, A, C);
-    uint64_t x = (A * drand48_seed(seed) + C) & kDrandMask;
-    const size_t last = first + kChunk < n ? first + kChunk : n;
-    for (size_t i = first; i < last; ++i) {
-        x = drand48_step(x);
-        spins[i] = (uint8_t)(x >> 47);
-    }
+    hot_start_chunk(n, seed, spins);
 }
 
 __global__ void k_fill(const size_t n, const uint8_t v, uint8_t *p)
@@ -489,7 +458,7 @@ int swb_create(swb_lattice **out, uint32_t L0, uint32_t L1, uint32_t tile_x, uin
     SWB_TRY(cudaMalloc(&h->rng_state, (size_t)h->n_tiles * h->W * sizeof(uint32_t)));
     SWB_TRY(cudaMalloc(&h->rng_sel, (size_t)h->n_tiles * h->W));
     SWB_TRY(cudaMalloc(&h->rng_iter, (size_t)h->n_tiles * sizeof(uint32_t)));
-    SWB_TRY(cudaMalloc(&h->edge, (size_t)h->n_blocks * edge_stride(h->g) * sizeof(uint32_t)));
+    SWB_TRY(cudaMalloc(&h->edge, (size_t)h->n_blocks * kEdgeWords * sizeof(uint32_t)));
     bool resolve = h->n_blocks >= kResolveMinBlocks || h->g.BX * h->g.BY >= kResolveBlockSites;
     if (const char *e = std::getenv("SWB_RESOLVE_MIN_BLOCKS"))
         resolve = h->n_blocks >= (uint32_t)std::strtoul(e, nullptr, 10);
@@ -1038,7 +1007,7 @@ int swb_update_host(swb_lattice *h, float temperature, const uint8_t *spins_in, 
 // pool already holds its whole HBM budget.  For such a caller a per-sweep cudaMalloc can fail
 // (the pool has the memory) and a cudaFree synchronises the whole device, stalling the other
 // lattices' streams.  The caller passes its spins and lcg32 streams; the sweep's scratch (label
-// array, block edge records, fault word) lives in one file-scope device array (sw_static_scratch.cu), which
+// array, block edge words, fault word) lives in one file-scope device array (sw_static_scratch.cu), which
 // every call on a device shares.
 
 namespace swb {
@@ -1083,7 +1052,7 @@ int swb_sweep_static(void *stream, uint32_t L0, uint32_t L1, uint32_t tile_x, ui
     h.smem_assign = assign_smem(h.g, h.W).total;
     h.smem_flip = flip_smem_bytes(h.g);
     const size_t labels_bytes = align256(h.n * sizeof(uint32_t) + 16);
-    const size_t edge_bytes = align256((size_t)h.n_blocks * edge_stride(h.g) * sizeof(uint32_t));
+    const size_t edge_bytes = align256((size_t)h.n_blocks * kEdgeWords * sizeof(uint32_t));
     if (labels_bytes + edge_bytes + 256 > kStaticScratchBytes)
         return fail(SWB_ERR_CAPACITY, "lattice %u x %u with tile %u x %u needs %zu bytes of scratch, the static array holds %zu",
                     L0, L1, tile_x, tile_y, labels_bytes + edge_bytes + 256, kStaticScratchBytes);
@@ -1100,7 +1069,7 @@ int swb_sweep_static(void *stream, uint32_t L0, uint32_t L1, uint32_t tile_x, ui
     h.edge = reinterpret_cast<uint32_t *>(base + labels_bytes);
     h.fault = reinterpret_cast<unsigned int *>(base + labels_bytes + edge_bytes);
 
-    // The array keeps the previous call's contents.  Labels and edge records are fully written by
+    // The array keeps the previous call's contents.  Labels and edge words are fully written by
     // the assign kernel before they are read; only the fault word must start at zero.
     SWB_CUDA(cudaMemsetAsync(h.fault, 0, sizeof(unsigned int), h.stream));
     const float p_add = swb_p_add(temperature);

@@ -3,7 +3,7 @@
 // device code, so every .cu file becomes its own device module, and a module's __device__
 // arrays are reserved on a device when that module loads there.  Here that happens only at the
 // first cudaGetSymbolAddress below, i.e. on a device where swb_sweep_static is called: the
-// other entry points never reserve these 26 MiB.
+// other entry points never reserve these 24 MiB + 1 KiB.
 
 #include <cuda_runtime.h>
 

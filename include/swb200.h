@@ -165,6 +165,44 @@ int swb_sweep_timed(swb_lattice *h, float temperature, uint32_t n_sweeps, int pe
 int swb_host_alloc(void **ptr, size_t bytes);
 int swb_host_free(void *ptr);
 
+/* ---- 3D: the Swendsen-Wang sweep of the 3D Ising model ------------------------------------ */
+/* No counterpart in the reference, which names the 3D case only
+ * (ising/include/swendsen_wang_selflabeling.hpp:20-22).  The 2D conventions extended to a
+ * periodic L0 x L1 x L2 lattice: spins uint8 0/1 at (z L1 + y) L0 + x; one lcg32 stream per
+ * tile of tile_x x tile_y x tile_z sites (tiles row-major), seeded seed_base + tile id; per tile
+ * and sweep the draws are, row by row (z-major), tile_x numbers for the +x bonds, then for the
+ * +y bonds of every row but the tile's last, then for the +z bonds of every layer but its last,
+ * then one request of tx tz + ty tz + tx ty numbers for its +y, +x and +z faces (the order of
+ * oracle/sw_oracle.c orc3_sw_sweep, which L2 = 1 reduces to the 2D sweep); labels are the
+ * minimum site index of each cluster and a cluster flips iff its label is odd. */
+typedef struct swb_lattice3 swb_lattice3;
+
+/* L0, L1 even, L2 even or 1; tile_x in {8, 16, 32}, 1 <= tile_y, tile_z <= 8; lcg_width in {8,
+ * 16, 32}.  Spins start all 0. */
+int swb3_create(swb_lattice3 **out, uint32_t L0, uint32_t L1, uint32_t L2, uint32_t tile_x, uint32_t tile_y,
+                uint32_t tile_z, uint32_t lcg_width, uint32_t seed_base, int device);
+int swb3_destroy(swb_lattice3 *h);
+/* geometry[0..11] = L0, L1, L2, tile x, y, z, block x, y, z (sites), blocks in x, y, z. */
+int swb3_geometry(swb_lattice3 *h, uint32_t *geometry);
+int swb3_set_spins(swb_lattice3 *h, const uint8_t *host_spins);
+int swb3_get_spins(swb_lattice3 *h, uint8_t *host_spins);
+/* Site i takes drand48 draw i + 1 after srand48(seed), as Lattice<2>'s hot start. */
+int swb3_hot_start(swb_lattice3 *h, uint32_t seed);
+/* n_sweeps sweeps; with measure_every > 0 e = sum s (s_x+ + s_y+ + s_z+) and m = sum s are
+ * recorded after every measure_every-th sweep (E/N = -e / N). */
+int swb3_sweep(swb_lattice3 *h, float temperature, uint32_t n_sweeps, uint32_t measure_every);
+/* One sweep with its bonds (bit 0 +x, 1 +y, 2 +z) and resolved labels dumped to host buffers
+ * (each may be NULL).  Synchronous. */
+int swb3_sweep_dumped(swb_lattice3 *h, float temperature, uint8_t *bonds, uint32_t *labels_final);
+/* n_sweeps sweeps timed with CUDA events on the handle's stream (ms of all of them). */
+int swb3_sweep_timed(swb_lattice3 *h, float temperature, uint32_t n_sweeps, float *ms);
+int swb3_energy_magnetization(swb_lattice3 *h, double *out, int64_t *e_sum, int64_t *m_sum);
+/* Recorded samples (e, m interleaved) and the accumulators (sum E/N, sum (E/N)^2, sum |M/N|,
+ * samples; acc may be NULL). */
+int swb3_samples(swb_lattice3 *h, int64_t *em, uint64_t capacity, uint64_t *count, double *acc);
+int swb3_rng_shape(swb_lattice3 *h, uint32_t *n_tiles, uint32_t *lcg_width);
+int swb3_get_rng(swb_lattice3 *h, uint32_t *state, uint32_t *a, uint32_t *c, uint32_t *iteration);
+
 /* ---- device memory and devices, for host programs that include no CUDA header ----------- */
 
 /* Makes the handle sweep a caller-owned spin array in device memory (L0*L1 bytes, 0/1,
@@ -214,8 +252,8 @@ int swb_update_host(swb_lattice *h, float temperature, const uint8_t *spins_in, 
  * current device: spins[L0*L1] (0/1, 16-byte aligned), rng_state[n_tiles*W], rng_sel[n_tiles*W]
  * (index 0..4 of the lcg32 parameter pair, random/src/lcg32.cpp:17-24), rng_iter[n_tiles],
  * n_tiles = ceil(L0/tile_x) * ceil(L1/tile_y) -- the layout swb_get_rng exports.  Results equal
- * swb_sweep's on the same state.  The label array, block edge records and fault word live in one
- * static device array of 26 MiB, so L0*L1 is at most 4,194,304 (2048 x 2048); larger
+ * swb_sweep's on the same state.  The label array, block edge words and fault word live in one
+ * static device array of 24 MiB + 1 KiB, so L0*L1 is at most 4,194,304 (2048 x 2048); larger
  * lattices return SWB_ERR_CAPACITY before any CUDA call.  All calls on a device share that array
  * (each call clears its fault word, the kernels overwrite the rest): calls that overlap on the
  * GPU race, so serialise them (one stream, or events).  The first call on each device looks the

@@ -85,6 +85,9 @@ class Oracle:
         lib.orc_sw_sweep.restype = ctypes.c_int
         lib.orc_energy_magnetization.argtypes = [_U, _U, _P, _P, _P]
         lib.orc_block_labels.argtypes = [_U, _U, _U, _U, _P, _P]
+        lib.orc3_sw_sweep.argtypes = [_U, _U, _U, _U, _U, _U, _U, _F, _P, _P, _P, _P, _P, _P, _P]
+        lib.orc3_sw_sweep.restype = ctypes.c_int
+        lib.orc3_energy_magnetization.argtypes = [_U, _U, _U, _P, _P, _P]
         self.lib = lib
 
     def hot_start(self, L0: int, L1: int, seed: int = 1) -> np.ndarray:
@@ -137,6 +140,27 @@ class Oracle:
         out = np.empty((L1, L0), np.uint32)
         self.lib.orc_block_labels(L0, L1, block_x, block_y, _ptr(b), _ptr(out))
         return out
+
+    def sweep3(self, spins: np.ndarray, tile: tuple[int, int, int], rng: RngTiles, T: float | None = None,
+               p_add: float | None = None, dumps: bool = False):
+        """One 3D sweep in place on spins [L2, L1, L0] (uint8); with dumps returns (bonds, labels)."""
+        L2, L1, L0 = spins.shape
+        p = self.p_add(T) if p_add is None else p_add
+        bonds = np.empty(spins.shape, np.uint8) if dumps else None
+        lab = np.empty(spins.shape, np.uint32) if dumps else None
+        rc = self.lib.orc3_sw_sweep(L0, L1, L2, tile[0], tile[1], tile[2], rng.W, p, _ptr(spins), _ptr(rng.state),
+                                    _ptr(rng.a), _ptr(rng.c), _ptr(rng.iteration), _ptr(bonds), _ptr(lab))
+        if rc != 0:
+            raise ValueError(f"orc3_sw_sweep failed with status {rc}")
+        return (bonds, lab) if dumps else None
+
+    def energy_magnetization3(self, spins: np.ndarray) -> tuple[int, int]:
+        L2, L1, L0 = spins.shape
+        e = ctypes.c_int64()
+        m = ctypes.c_int64()
+        s = np.ascontiguousarray(spins, np.uint8)
+        self.lib.orc3_energy_magnetization(L0, L1, L2, _ptr(s), ctypes.byref(e), ctypes.byref(m))
+        return e.value, m.value
 
     def energy_magnetization(self, spins: np.ndarray) -> tuple[int, int]:
         L1, L0 = spins.shape

@@ -267,3 +267,139 @@ void orc_block_labels(uint32_t L0, uint32_t L1, uint32_t BX, uint32_t BY, const 
     for (size_t s = 0; s < n; ++s)
         out[s] = uf_find(out, (uint32_t)s);
 }
+
+/* ---- 3D Swendsen-Wang (this project's extension; the reference names it only in a comment,
+ * ising/include/swendsen_wang_selflabeling.hpp:20-22).  Periodic L0 x L1 x L2, site index
+ * (z L1 + y) L0 + x, tiles tx x ty x tz in row-major tile order, one lcg32 stream per tile.  Per
+ * tile and sweep the draws extend the 2D order: per (kk, jj) row a request of tx numbers for the
+ * +x bonds (the row's last site bonds through the face request), then per row with jj + 1 <
+ * jj_max one for the +y bonds, then per row with kk + 1 < kk_max one for the +z bonds, then one
+ * face request of tx tz + ty tz + tx ty numbers: the +y face (element kk tx + ii, the tile's last
+ * row), the +x face (tx tz + kk ty + jj, its last column), the +z face (tx tz + ty tz + jj tx + ii,
+ * its last layer), each to the periodic neighbour.  Rows run kk-major, then jj.  A bond needs
+ * equal spins and an accepted draw; labels are the minimum site index of each cluster; a
+ * cluster flips iff its label is odd.  With L2 = tz = 1 the bonds, labels and flips of a sweep
+ * are the 2D sweep's (the face request begins with the 2D merge request; the z bonds join a site
+ * to itself), which pins this restatement to the 2D one. */
+int orc3_sw_sweep(uint32_t L0, uint32_t L1, uint32_t L2, uint32_t tx, uint32_t ty, uint32_t tz, uint32_t W,
+                  float p_add, uint8_t *spins, uint32_t *rng_state, uint32_t *rng_a, uint32_t *rng_c,
+                  uint32_t *rng_iteration, uint8_t *bonds, uint32_t *labels_final)
+{
+    if (L0 % 2 || L1 % 2 || (L2 % 2 && L2 != 1))
+        return 1;
+    if (!valid_width(W))
+        return 2;
+    const size_t plane = (size_t)L0 * L1, n = plane * L2;
+    const uint32_t n0 = (L0 + tx - 1) / tx, n1 = (L1 + ty - 1) / ty, n2 = (L2 + tz - 1) / tz;
+    const uint32_t nface = tx * tz + ty * tz + tx * ty;
+    uint8_t *bond = (uint8_t *)calloc(n, 1);
+    uint32_t *parent = (uint32_t *)malloc(n * sizeof(uint32_t));
+    float *row = (float *)malloc((size_t)(nface > tx ? nface : tx) * sizeof(float));
+    if (!bond || !parent || !row) {
+        free(bond); free(parent); free(row);
+        return 3;
+    }
+#define SITE(x, y, z) (((size_t)(z) * L1 + (y)) * L0 + (x))
+    for (uint32_t t = 0; t < n0 * n1 * n2; ++t) {
+        uint32_t *st = rng_state + (size_t)t * W, *aa = rng_a + (size_t)t * W, *cc = rng_c + (size_t)t * W;
+        uint32_t *it = rng_iteration + t;
+        const uint32_t i = (t % n0) * tx, j = ((t / n0) % n1) * ty, k = (t / (n0 * n1)) * tz;
+        const uint32_t ii_max = tx < L0 - i ? tx : L0 - i;
+        const uint32_t jj_max = ty < L1 - j ? ty : L1 - j;
+        const uint32_t kk_max = tz < L2 - k ? tz : L2 - k;
+        for (uint32_t kk = 0; kk < kk_max; ++kk)
+            for (uint32_t jj = 0; jj < jj_max; ++jj) {
+                orc_lcg32_next_real(W, st, aa, cc, it, tx, row);
+                for (uint32_t ii = 0; ii + 1 < ii_max; ++ii) {
+                    const size_t s = SITE(i + ii, j + jj, k + kk);
+                    if (spins[s] == spins[s + 1] && row[ii] < p_add)
+                        bond[s] |= 1;
+                }
+            }
+        for (uint32_t kk = 0; kk < kk_max; ++kk)
+            for (uint32_t jj = 0; jj + 1 < jj_max; ++jj) {
+                orc_lcg32_next_real(W, st, aa, cc, it, tx, row);
+                for (uint32_t ii = 0; ii < ii_max; ++ii) {
+                    const size_t s = SITE(i + ii, j + jj, k + kk);
+                    if (spins[s] == spins[s + L0] && row[ii] < p_add)
+                        bond[s] |= 2;
+                }
+            }
+        for (uint32_t kk = 0; kk + 1 < kk_max; ++kk)
+            for (uint32_t jj = 0; jj < jj_max; ++jj) {
+                orc_lcg32_next_real(W, st, aa, cc, it, tx, row);
+                for (uint32_t ii = 0; ii < ii_max; ++ii) {
+                    const size_t s = SITE(i + ii, j + jj, k + kk);
+                    if (spins[s] == spins[s + plane] && row[ii] < p_add)
+                        bond[s] |= 4;
+                }
+            }
+        orc_lcg32_next_real(W, st, aa, cc, it, nface, row);
+        for (uint32_t kk = 0; kk < kk_max; ++kk)
+            for (uint32_t ii = 0; ii < ii_max; ++ii) {
+                const size_t s = SITE(i + ii, j + jj_max - 1, k + kk);
+                const size_t s2 = SITE(i + ii, (j + jj_max) % L1, k + kk);
+                if (row[kk * tx + ii] < p_add && spins[s] == spins[s2])
+                    bond[s] |= 2;
+            }
+        for (uint32_t kk = 0; kk < kk_max; ++kk)
+            for (uint32_t jj = 0; jj < jj_max; ++jj) {
+                const size_t s = SITE(i + ii_max - 1, j + jj, k + kk);
+                const size_t s2 = SITE((i + ii_max) % L0, j + jj, k + kk);
+                if (row[tx * tz + kk * ty + jj] < p_add && spins[s] == spins[s2])
+                    bond[s] |= 1;
+            }
+        for (uint32_t jj = 0; jj < jj_max; ++jj)
+            for (uint32_t ii = 0; ii < ii_max; ++ii) {
+                const size_t s = SITE(i + ii, j + jj, k + kk_max - 1);
+                const size_t s2 = SITE(i + ii, j + jj, (k + kk_max) % L2);
+                if (row[tx * tz + ty * tz + jj * tx + ii] < p_add && spins[s] == spins[s2])
+                    bond[s] |= 4;
+            }
+    }
+    if (bonds)
+        memcpy(bonds, bond, n);
+    for (size_t s = 0; s < n; ++s)
+        parent[s] = (uint32_t)s;
+    for (uint32_t z = 0; z < L2; ++z)
+        for (uint32_t y = 0; y < L1; ++y)
+            for (uint32_t x = 0; x < L0; ++x) {
+                const size_t s = SITE(x, y, z);
+                if (bond[s] & 1)
+                    uf_union(parent, (uint32_t)s, (uint32_t)SITE((x + 1) % L0, y, z));
+                if (bond[s] & 2)
+                    uf_union(parent, (uint32_t)s, (uint32_t)SITE(x, (y + 1) % L1, z));
+                if (bond[s] & 4)
+                    uf_union(parent, (uint32_t)s, (uint32_t)SITE(x, y, (z + 1) % L2));
+            }
+    for (size_t s = 0; s < n; ++s) {
+        const uint32_t r = uf_find(parent, (uint32_t)s);
+        if (labels_final)
+            labels_final[s] = r;
+        spins[s] ^= (uint8_t)(r & 1u);
+    }
+#undef SITE
+    free(bond);
+    free(parent);
+    free(row);
+    return 0;
+}
+
+/* e = sum s (s_x+ + s_y+ + s_z+), m = sum s over the periodic L0 x L1 x L2 lattice, s = 2b - 1. */
+void orc3_energy_magnetization(uint32_t L0, uint32_t L1, uint32_t L2, const uint8_t *spins, int64_t *e, int64_t *m)
+{
+    int64_t ee = 0, mm = 0;
+    for (uint32_t z = 0; z < L2; ++z)
+        for (uint32_t y = 0; y < L1; ++y)
+            for (uint32_t x = 0; x < L0; ++x) {
+                const size_t s = ((size_t)z * L1 + y) * L0 + x;
+                const int v = 2 * spins[s] - 1;
+                const int rx = 2 * spins[((size_t)z * L1 + y) * L0 + (x + 1) % L0] - 1;
+                const int ry = 2 * spins[((size_t)z * L1 + (y + 1) % L1) * L0 + x] - 1;
+                const int rz = 2 * spins[((size_t)((z + 1) % L2) * L1 + y) * L0 + x] - 1;
+                ee += v * (rx + ry + rz);
+                mm += v;
+            }
+    *e = ee;
+    *m = mm;
+}

@@ -73,6 +73,13 @@ void orc_energy_magnetization(uint32_t L0, uint32_t L1, const uint8_t *spins, in
  * blocks in place of tiles. */
 void orc_block_labels(uint32_t L0, uint32_t L1, uint32_t BX, uint32_t BY, const uint8_t *bonds, uint32_t *out);
 
+/* 3D Swendsen-Wang sweep (the draw order is described in sw_oracle.c; L2 = 1 gives the 2D sweep)
+ * and its energy / magnetisation sums. */
+int orc3_sw_sweep(uint32_t L0, uint32_t L1, uint32_t L2, uint32_t tx, uint32_t ty, uint32_t tz, uint32_t W,
+                  float p_add, uint8_t *spins, uint32_t *rng_state, uint32_t *rng_a, uint32_t *rng_c,
+                  uint32_t *rng_iteration, uint8_t *bonds, uint32_t *labels_final);
+void orc3_energy_magnetization(uint32_t L0, uint32_t L1, uint32_t L2, const uint8_t *spins, int64_t *e, int64_t *m);
+
 #ifdef __cplusplus
 }
 #endif
