@@ -257,12 +257,12 @@ def assign_bytes(n_sites: int, n_tiles: int, W: int) -> float:
 
 # DRAM traffic of one assign pass over a workload (dram__bytes_read.sum + dram__bytes_write.sum)
 # from one ncu capture of the same kernel, per site: the batched mix of 512 lattices (39,603,200
-# sites; the round runs its two lattice groups as two launches: 33,100,288 + 33,114,624 B read,
-# 38,437,632 + 40,070,912 B written) and one 8192 x 8192 lattice, tile 16 x 8 (111,201,792 B read
-# + 254,913,792 B written).  Traffic grows with the sites swept, so other sizes scale by their
+# sites; the round runs its two lattice groups as two launches: 33,099,264 + 33,123,584 B read,
+# 36,406,016 + 41,822,720 B written) and one 8192 x 8192 lattice, tile 16 x 8 (111,227,136 B read
+# + 253,618,688 B written).  Traffic grows with the sites swept, so other sizes scale by their
 # site count.
-ASSIGN_TRAFFIC_PER_SITE = {"kb_assign": (33_100_288 + 33_114_624 + 38_437_632 + 40_070_912) / 39_603_200,
-                           "k_assign": (111_201_792 + 254_913_792) / 8192 ** 2}
+ASSIGN_TRAFFIC_PER_SITE = {"kb_assign": (33_099_264 + 33_123_584 + 36_406_016 + 41_822_720) / 39_603_200,
+                           "k_assign": (111_227_136 + 253_618_688) / 8192 ** 2}
 
 
 def flip_bytes(n_sites: int) -> float:
