@@ -255,8 +255,12 @@ struct AssignDump {
 };
 
 struct AssignSmem {
-    uint32_t parent, draws, slots, edge, bond, sp, plab, total, pitch;
+    uint32_t parent, draws, slots, edge, bond, sp, plab, pairs, total, pitch;
 };
+
+// Pending unions of the scanline labelling (row path): 2048 words shared by the CTA's warps
+// (64 per warp at 1024 threads, 128 at 512), one uint16 pair per word.
+constexpr uint32_t kPairWords = 2048;
 
 // Updates of every lcg32 lane in one sweep: 2 tile_y - 1 row requests of tile_x numbers and
 // the merge request of tile_x + tile_y numbers, W numbers per update.
@@ -277,7 +281,8 @@ __host__ __device__ inline AssignSmem assign_smem(const Geo &g, uint32_t W)
     s.bond = s.edge + kEdgeWords * 4;
     s.sp = (s.bond + ns + 15) & ~15u;
     s.plab = (s.sp + (g.BY + 1) * s.pitch + 15) & ~15u;  // uint16 provisional labels (row path)
-    s.total = (s.plab + 2 * ns + 15) & ~15u;
+    s.pairs = (s.plab + 2 * ns + 15) & ~15u;
+    s.total = s.pairs + kPairWords * 4;
     return s;
 }
 
@@ -522,6 +527,22 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
     const uint32_t rb = (nb & (nb - 1)) == 0 ? (BY + nb - 1) >> (__ffs(nb) - 1)  // rows per band
                                              : (BY + nb - 1) / nb;
     const uint32_t below = (1u << lane) - 1u;                // lanes below this one
+    // The unions a band needs are queued in the warp's slice of the pair list and run together,
+    // one per lane (a union inside the row step would run, divergent, on almost every row).
+    // Deferring them changes no provisional label, and the union-find's roots (each set's
+    // minimum) do not depend on the order of the unions.
+    const uint32_t pcap = kThreads ? kPairWords / (kThreads / 32) : kPairWords / nwarps;  // >= 64
+    uint32_t *pl = reinterpret_cast<uint32_t *>(smem + L.pairs) + warp * pcap;
+    uint32_t npend = 0;  // queued pairs (warp-uniform)
+    auto flush = [&]() {
+        __syncwarp();
+        for (uint32_t i = lane; i < npend; i += 32) {
+            const uint32_t pr = pl[i];
+            uf_union(parent, pr & 0xFFFFu, pr >> 16);
+        }
+        __syncwarp();
+        npend = 0;
+    };
     // One row of a band: `above` holds the provisional label of the site above, Yup the row
     // above's y-bond word, Xa its x-bond word.
     auto row = [&](const uint32_t X, const uint32_t base, uint32_t &above, const uint32_t Yup, const uint32_t Xa) {
@@ -534,8 +555,13 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
         // A y-bond whose left neighbour is bonded up too, with both rows bonded across, meets
         // the same two runs as that neighbour's: only the leftmost of such a chain unites.
         const uint32_t U = Yup & ~((Yup & X & Xa) << 1);
-        if (((U >> lane) & 1u) && above != lab)
-            uf_union(parent, above, lab);
+        const bool need = ((U >> lane) & 1u) && above != lab;
+        const uint32_t m = __ballot_sync(0xffffffffu, need);
+        if (need)
+            pl[npend + __popc(m & below)] = above | lab << 16;
+        npend += __popc(m);
+        if (npend > pcap - 32)  // room for the next row's pairs
+            flush();
         plab[base + lane] = (uint16_t)lab;
         above = lab;
     };
@@ -554,6 +580,7 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
             Xa = X;
             Yup = xp[kBY * kNW + r * kNW];
         }
+        flush();
     } else {
         for (uint32_t task = warp; task < NW * nb; task += nwarps) {
             const uint32_t sx = task & (NW - 1), band = task >> lnw;
@@ -569,6 +596,7 @@ __device__ __forceinline__ void assign_block_labels_rows(const Geo &g, const uin
                 xp += NW;
                 base += BX;
             }
+            flush();
         }
     }
     __syncthreads();
