@@ -576,18 +576,25 @@ def bench_batched(args, dist: Dist, cp) -> dict:
     ab = assign_bytes(sites, n_tiles, 16)
     peak, peak_kind = hbm_peak()
     # e2e: every step copies all spins in from pinned host memory and back out; the lattices'
-    # host buffers are consecutive slices of one pinned arena per direction (BatchedSW.host_io)
+    # host buffers are consecutive slices of one pinned arena per direction (BatchedSW.host_io).
+    # The steps run as one pipelined call (update_host_io_rounds: a lattice group's next copy in
+    # starts once its copy out has landed); one call per step is timed beside it.
     io = b.host_io(ids)
     for lid, x in zip(ids, io.inputs):
         x[:] = b.get_spins(lid)
     b.update_host_io(io)
     io.swap()
+    b.update_host_io_rounds(io, 2)
     e2e_steps = max(3, min(args.steps, 20))
     dist.barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         b.update_host_io(io)
         io.swap()
+    e2e_sync_s = dist.max(time.perf_counter() - t0)
+    dist.barrier()
+    t0 = time.perf_counter()
+    b.update_host_io_rounds(io, e2e_steps)
     e2e_s = dist.max(time.perf_counter() - t0)
     # per-lattice observables of the final state, gathered on rank 0 (control plane only)
     merged = shard.gather_results(mix_observables(b, ids, mine), dist.gather_object)
@@ -600,7 +607,9 @@ def bench_batched(args, dist: Dist, cp) -> dict:
                      "bytes_per_launch": ab, "ms_per_launch": a_ms},
         "kernels_ms_per_sweep": {"assign": a_ms, "merge": float(k[2]) / nk, "resolve_flip": float(k[3]) / nk},
         "e2e": {"value": sites_all * e2e_steps / e2e_s, "unit": "spin-updates/s",
-                "h2d_bytes_per_step": sites_all, "d2h_bytes_per_step": sites_all},
+                "h2d_bytes_per_step": sites_all, "d2h_bytes_per_step": sites_all,
+                "api": "swb_batch_update_host_rounds: the steps as one pipelined call through two pinned host arenas",
+                "one_step_per_call": sites_all * e2e_steps / e2e_sync_s},
         "tiles": {str(L): [list(t), list(bl)] for (L, _, _), (t, bl) in sorted(zip(mix, tiles))},
         "autotune_table": table.get("device", "none"),
     }

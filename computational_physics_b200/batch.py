@@ -34,6 +34,7 @@ extra_signatures({
     "swb_batch_info": ([P, U32, P], I32),
     "swb_batch_memory": ([P, P, P], I32),
     "swb_batch_update_host": ([P, U32, P, P, P], I32),
+    "swb_batch_update_host_rounds": ([P, U32, P, P, P, U32], I32),
 })
 
 UNLIMITED = 0xFFFFFFFF
@@ -239,6 +240,16 @@ class BatchedSW:
         """update_host with the buffers of `io` (io.inputs in, io.outputs out), one copy per
         direction through the arenas and no per-call pointer work in Python."""
         check(self._lib.swb_batch_update_host(self._h, io.count, io._ids.ctypes.data, io._pin, io._pout))
+
+    def update_host_io_rounds(self, io: "HostIO", rounds: int) -> None:
+        """`rounds` rounds of update_host_io with io.swap() after each, as one pipeline: every
+        round copies all of io's lattices in and out, and a lattice group's next copy in starts
+        as soon as its copy out has landed.  Afterwards io.inputs holds the last round's
+        spins."""
+        check(self._lib.swb_batch_update_host_rounds(self._h, io.count, io._ids.ctypes.data, io._pin, io._pout,
+                                                     int(rounds)))
+        if rounds % 2:
+            io.swap()
 
 
 class HostIO:

@@ -1172,15 +1172,23 @@ int swb_batch_memory(swb_batch *b, uint64_t *used, uint64_t *budget)
     return SWB_OK;
 }
 
-int swb_batch_update_host(swb_batch *b, uint32_t count, const uint32_t *ids, const uint8_t *const *spins_in,
-                          uint8_t *const *spins_out)
+}  // extern "C"
+
+namespace {
+
+// n_rounds rounds through host buffers: round r copies spins in from side r % 2 (0: spins_in,
+// 1: spins_out), sweeps every lattice once and copies the spins out to the other side.
+int update_host_rounds(swb_batch *b, uint32_t count, const uint32_t *ids, const uint8_t *const *spins_in,
+                       uint8_t *const *spins_out, const uint32_t n_rounds)
 {
     if (!b || (count && (!ids || !spins_in || !spins_out)))
         return fail(SWB_ERR_ARGUMENT, "NULL argument");
     if (int rc = bset_device(b))
         return rc;
+    if (n_rounds == 0)
+        return SWB_OK;
     if (count == 0) {
-        if (int rc = rounds(b, 1, false))
+        if (int rc = rounds(b, n_rounds, false))
             return rc;
         SWB_CUDA(cudaStreamSynchronize(b->stream));
         return SWB_OK;
@@ -1189,7 +1197,10 @@ int swb_batch_update_host(swb_batch *b, uint32_t count, const uint32_t *ids, con
     // groups of about equal bytes that form a pipeline: group g's host-to-device copies (one
     // per run of host buffers that follow each other in memory) overlap the sweep of group
     // g - 1 and the device-to-host copies of group g - 2, on three streams.  Lattices that are
-    // not listed are swept first, while the first group's spins are still on their way.
+    // not listed are swept first, while the first group's spins are still on their way.  Over
+    // several rounds the pipeline runs on without a host synchronisation: group g's copies in
+    // for round r wait only for its copies out of round r - 1 (the host buffers they read and
+    // the staging bytes they overwrite).
     if (int rc = rebuild_lists(b))
         return rc;
     auto &P = b->io;
@@ -1213,7 +1224,7 @@ int swb_batch_update_host(swb_batch *b, uint32_t count, const uint32_t *ids, con
         }
         // groups [gs[g], gs[g + 1]) of listed lattices and their block items; the unlisted
         // active lattices' items come first
-        constexpr uint32_t kGroups = 4;  // measured: 4 groups beat 8, 12 and 16 (each group costs ~35 us of dependencies)
+        constexpr uint32_t kGroups = 8;  // measured on the 512-lattice mix: 6 to 8 groups beat 2, 4, 10, 12 and 16
         const uint32_t G = std::min(count, kGroups);
         std::vector<uint32_t> gs(G + 1, count);
         gs[0] = 0;
@@ -1285,53 +1296,61 @@ int swb_batch_update_host(swb_batch *b, uint32_t count, const uint32_t *ids, con
         SWB_CUDA(cudaStreamCreateWithFlags(&b->s_in, cudaStreamNonBlocking));
     if (!b->s_out)
         SWB_CUDA(cudaStreamCreateWithFlags(&b->s_out, cudaStreamNonBlocking));
-    while (b->io_events.size() < 2 * G) {  // [g]: group g staged; [G + g]: group g swept
+    while (b->io_events.size() < 3 * G) {  // [g]: group g staged; [G + g]: swept; [2G + g]: copied out
         cudaEvent_t e;
         SWB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         b->io_events.push_back(e);
     }
     cudaEvent_t *ev = b->io_events.data();
     auto run = [&]() -> int {
-        kb_begin_round<<<4, 128, 0, b->stream>>>(b->d_lats, b->d_active, b->d_ctr);
-        SWB_LAUNCHED();
-        if (gi[1])
-            if (int rc = launch_phases_b(b, b->d_io_items, (uint32_t)gi[1], b->stream))
-                return rc;
-        for (uint32_t g = 0; g < G; ++g) {
-            for (uint32_t k = gs[g]; k < gs[g + 1];) {
-                uint32_t j = k + 1;
-                while (j < gs[g + 1] && spins_in[j] == spins_in[j - 1] + copies[j - 1].bytes)
-                    ++j;
-                SWB_CUDA(cudaMemcpyAsync(b->d_stage + copies[k].offset, spins_in[k],
-                                         copies[j - 1].offset + copies[j - 1].bytes - copies[k].offset,
-                                         cudaMemcpyHostToDevice, b->s_in));
-                k = j;
-            }
-            SWB_CUDA(cudaEventRecord(ev[g], b->s_in));
-        }
-        for (uint32_t g = 0; g < G; ++g) {
-            const uint32_t n = gs[g + 1] - gs[g];
-            SWB_CUDA(cudaStreamWaitEvent(b->stream, ev[g], 0));
-            const dim3 sgrid((uint32_t)((P.max_bytes[g] + kStagePiece - 1) / kStagePiece), n);
-            kb_stage_copy<<<sgrid, 256, 0, b->stream>>>(b->d_copies + gs[g], b->d_stage, 1);
+        for (uint32_t r = 0; r < n_rounds; ++r) {
+            const uint8_t *const *src = (r & 1) ? spins_out : spins_in;
+            uint8_t *const *dst = (r & 1) ? const_cast<uint8_t *const *>(spins_in) : spins_out;
+            kb_begin_round<<<4, 128, 0, b->stream>>>(b->d_lats, b->d_active, b->d_ctr);
             SWB_LAUNCHED();
-            if (int rc = launch_phases_b(b, b->d_io_items + gi[g + 1], (uint32_t)(gi[g + 2] - gi[g + 1]), b->stream))
-                return rc;
-            kb_stage_copy<<<sgrid, 256, 0, b->stream>>>(b->d_copies + gs[g], b->d_stage, 0);
-            SWB_LAUNCHED();
-            if (g + 1 == G)  // every listed and unlisted lattice has swept: close the round
-                if (int rc = launch_end_round(b, b->stream, false))
+            if (gi[1])
+                if (int rc = launch_phases_b(b, b->d_io_items, (uint32_t)gi[1], b->stream))
                     return rc;
-            SWB_CUDA(cudaEventRecord(ev[G + g], b->stream));
-            SWB_CUDA(cudaStreamWaitEvent(b->s_out, ev[G + g], 0));
-            for (uint32_t k = gs[g]; k < gs[g + 1];) {
-                uint32_t j = k + 1;
-                while (j < gs[g + 1] && spins_out[j] == spins_out[j - 1] + copies[j - 1].bytes)
-                    ++j;
-                SWB_CUDA(cudaMemcpyAsync(spins_out[k], b->d_stage + copies[k].offset,
-                                         copies[j - 1].offset + copies[j - 1].bytes - copies[k].offset,
-                                         cudaMemcpyDeviceToHost, b->s_out));
-                k = j;
+            for (uint32_t g = 0; g < G; ++g) {
+                if (r)  // the previous round's copies out of this group have landed
+                    SWB_CUDA(cudaStreamWaitEvent(b->s_in, ev[2 * G + g], 0));
+                for (uint32_t k = gs[g]; k < gs[g + 1];) {
+                    uint32_t j = k + 1;
+                    while (j < gs[g + 1] && src[j] == src[j - 1] + copies[j - 1].bytes)
+                        ++j;
+                    SWB_CUDA(cudaMemcpyAsync(b->d_stage + copies[k].offset, src[k],
+                                             copies[j - 1].offset + copies[j - 1].bytes - copies[k].offset,
+                                             cudaMemcpyHostToDevice, b->s_in));
+                    k = j;
+                }
+                SWB_CUDA(cudaEventRecord(ev[g], b->s_in));
+            }
+            for (uint32_t g = 0; g < G; ++g) {
+                const uint32_t n = gs[g + 1] - gs[g];
+                SWB_CUDA(cudaStreamWaitEvent(b->stream, ev[g], 0));
+                const dim3 sgrid((uint32_t)((P.max_bytes[g] + kStagePiece - 1) / kStagePiece), n);
+                kb_stage_copy<<<sgrid, 256, 0, b->stream>>>(b->d_copies + gs[g], b->d_stage, 1);
+                SWB_LAUNCHED();
+                if (int rc = launch_phases_b(b, b->d_io_items + gi[g + 1], (uint32_t)(gi[g + 2] - gi[g + 1]),
+                                             b->stream))
+                    return rc;
+                kb_stage_copy<<<sgrid, 256, 0, b->stream>>>(b->d_copies + gs[g], b->d_stage, 0);
+                SWB_LAUNCHED();
+                if (g + 1 == G)  // every listed and unlisted lattice has swept: close the round
+                    if (int rc = launch_end_round(b, b->stream, false))
+                        return rc;
+                SWB_CUDA(cudaEventRecord(ev[G + g], b->stream));
+                SWB_CUDA(cudaStreamWaitEvent(b->s_out, ev[G + g], 0));
+                for (uint32_t k = gs[g]; k < gs[g + 1];) {
+                    uint32_t j = k + 1;
+                    while (j < gs[g + 1] && dst[j] == dst[j - 1] + copies[j - 1].bytes)
+                        ++j;
+                    SWB_CUDA(cudaMemcpyAsync(dst[k], b->d_stage + copies[k].offset,
+                                             copies[j - 1].offset + copies[j - 1].bytes - copies[k].offset,
+                                             cudaMemcpyDeviceToHost, b->s_out));
+                    k = j;
+                }
+                SWB_CUDA(cudaEventRecord(ev[2 * G + g], b->s_out));
             }
         }
         SWB_CUDA(cudaStreamSynchronize(b->s_out));
@@ -1346,6 +1365,22 @@ int swb_batch_update_host(swb_batch *b, uint32_t count, const uint32_t *ids, con
         cudaStreamSynchronize(b->stream);
     }
     return rc ? rc : bcheck_fault(b);
+}
+
+}  // namespace
+
+extern "C" {
+
+int swb_batch_update_host(swb_batch *b, uint32_t count, const uint32_t *ids, const uint8_t *const *spins_in,
+                          uint8_t *const *spins_out)
+{
+    return update_host_rounds(b, count, ids, spins_in, spins_out, 1);
+}
+
+int swb_batch_update_host_rounds(swb_batch *b, uint32_t count, const uint32_t *ids, uint8_t *const *spins_a,
+                                 uint8_t *const *spins_b, uint32_t n_rounds)
+{
+    return update_host_rounds(b, count, ids, spins_a, spins_b, n_rounds);
 }
 
 }  // extern "C"

@@ -368,6 +368,16 @@ int swb_batch_memory(swb_batch *b, uint64_t *used, uint64_t *budget);
 int swb_batch_update_host(swb_batch *b, uint32_t count, const uint32_t *ids, const uint8_t *const *spins_in,
                           uint8_t *const *spins_out);
 
+/* n_rounds rounds of swb_batch_update_host that hand the spins back and forth between two sets
+ * of host buffers: round r copies in from spins_a when r is even (spins_b when odd), sweeps
+ * every lattice once and copies out to the other set, so after an odd number of rounds the
+ * spins are in spins_b, after an even number in spins_a.  Every round moves all listed
+ * lattices' spins in and out of the device; the rounds form one pipeline (a group of lattices
+ * starts its next round's copy in as soon as its copy out has landed) with one synchronisation
+ * at the end.  Synchronous. */
+int swb_batch_update_host_rounds(swb_batch *b, uint32_t count, const uint32_t *ids, uint8_t *const *spins_a,
+                                 uint8_t *const *spins_b, uint32_t n_rounds);
+
 #ifdef __cplusplus
 }
 #endif

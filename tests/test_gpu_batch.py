@@ -211,6 +211,31 @@ def test_host_io_steps(gpu, oracle):
         assert np.array_equal(b.get_spins(extra), want_x)
 
 
+@pytest.mark.parametrize("rounds", [1, 2, 5])
+def test_host_io_rounds(gpu, oracle, rounds):
+    """update_host_io_rounds: the pipelined rounds through the two HostIO arenas give the
+    oracle's sweeps, with the final spins in io.inputs, and lattices not in the HostIO sweep
+    once per round too."""
+    shapes = [((64, 64), (16, 8), 2.2, 21), ((34, 30), (16, 4), 2.5, 22), ((128, 96), (8, 8), 2.3, 23),
+              ((256, 256), (16, 8), 2.27, 24), ((96, 64), (16, 8), 2.4, 25)]
+    with gpu.BatchedSW(capacity=8) as b:
+        ids = [b.add(L0, L1, T, seed, tile) for (L0, L1), tile, T, seed in shapes]
+        extra = b.add(32, 32, 2.1, 26, (16, 8))
+        start_x = oracle.hot_start(32, 32, 26)
+        b.set_spins(extra, start_x)
+        io = b.host_io(ids)
+        starts = []
+        for x, ((L0, L1), _, _, seed) in zip(io.inputs, shapes):
+            x[:] = oracle.hot_start(L0, L1, seed)
+            starts.append(np.array(x))
+        b.update_host_io_rounds(io, rounds)
+        for x, start, (_, tile, T, seed) in zip(io.inputs, starts, shapes):
+            want, _ = _oracle_run(oracle, start, tile, T, seed, rounds)
+            assert np.array_equal(x, want)
+        want_x, _ = _oracle_run(oracle, start_x, (16, 8), 2.1, 26, rounds)
+        assert np.array_equal(b.get_spins(extra), want_x)
+
+
 def test_snapshot_resume_bit_identical(gpu, tmp_path):
     """Preempt a job (snapshot to disk), resume it in another batch and another slot, and in a
     single-lattice handle: every continuation equals the uninterrupted run."""
