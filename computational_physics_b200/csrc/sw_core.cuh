@@ -1003,7 +1003,8 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
 }
 
 // assign_block with the tile shape as compile-time constants for the common shapes (lcg width
-// 16), the runtime form otherwise.
+// 16), the runtime form otherwise; full 128 x 32 blocks of 16 x 8 tiles take the fixed-shape
+// scanline.
 template <int W>
 __device__ __forceinline__ void assign_block_any(const Geo &g, const uint32_t bxi, const uint32_t byi,
                                                  const uint8_t *__restrict__ spins, uint32_t *__restrict__ labels,
@@ -1013,8 +1014,9 @@ __device__ __forceinline__ void assign_block_any(const Geo &g, const uint32_t bx
 {
 #define SWB_TILE(tx, ty)                                                                                              \
     if (g.TX == tx && g.TY == ty) {                                                                                   \
-        assign_block<W, tx, ty, true, false>(g, bxi, byi, spins, labels, rng_state, rng_sel, rng_iter, thr, edge,   \
-                                             AssignDump{}, MeasureArgs{}, smem);                                      \
+        assign_block<W, tx, ty, true, false, tx == 16 && ty == 8>(g, bxi, byi, spins, labels, rng_state, rng_sel,    \
+                                                                 rng_iter, thr, edge, AssignDump{}, MeasureArgs{},   \
+                                                                 smem);                                              \
         return;                                                                                                       \
     }
     if constexpr (W == 16) {
