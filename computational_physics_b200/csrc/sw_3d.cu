@@ -325,7 +325,7 @@ __global__ void __launch_bounds__(k3Threads) k3_merge(const Geo3 g, const uint32
             const size_t nb = ((size_t)nz * g.L1 + ny) * g.L0 + nx;
             const uint32_t a = label_global3(g, bxi, byi, bzi, vl[s]), b = label_global3(g, nbx, nby, nbz, vl[nb]);
             if (a != b)
-                link = guf_union_pair(labels, a, b, fault);
+                link = guf_union_pair(labels, a, b, g.L0 * g.L1 * g.L2, fault);
         }
         linked[blk * nf + t] = link;
     }
@@ -339,7 +339,7 @@ __global__ void __launch_bounds__(k3Threads) k3_resolve(const Geo3 g, const uint
     for (uint32_t t = threadIdx.x; t < nf; t += blockDim.x) {
         const uint32_t b = linked[blk * nf + t];
         if (b != kNoLink)
-            labels[b] = guf_find(labels, b, fault);
+            labels[b] = guf_find(labels, b, g.L0 * g.L1 * g.L2, fault);
     }
 }
 
@@ -465,7 +465,7 @@ int check_fault3(swb_lattice3 *h)
     SWB_CUDA(cudaMemcpyAsync(&f, h->fault, sizeof(f), cudaMemcpyDeviceToHost, h->stream));
     SWB_CUDA(cudaStreamSynchronize(h->stream));
     if (f)
-        return fail(SWB_ERR_STATE, "label chase exceeded %u steps (fault word %u)", kChainCap, f);
+        return fail(SWB_ERR_STATE, "label union-find fault (word %u: 1 chain over %u steps, 2 union retries, 4 label outside the lattice)", f, kChainCap);
     return SWB_OK;
 }
 

@@ -366,7 +366,7 @@ int bcheck_fault(swb_batch *b)
     SWB_CUDA(cudaMemcpyAsync(&f, b->d_fault, sizeof(f), cudaMemcpyDeviceToHost, b->stream));
     SWB_CUDA(cudaStreamSynchronize(b->stream));
     if (f)
-        return fail(SWB_ERR_STATE, "label chase exceeded %u steps (fault word %u)", kChainCap, f);
+        return fail(SWB_ERR_STATE, "label union-find fault (word %u: 1 chain over %u steps, 2 union retries, 4 label outside the lattice)", f, kChainCap);
     return SWB_OK;
 }
 

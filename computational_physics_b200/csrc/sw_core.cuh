@@ -1068,7 +1068,7 @@ __device__ __forceinline__ void merge_block(const Geo &g, const uint32_t bxi, co
         const volatile uint32_t *vl = labels;
         const uint32_t a = label_global(g, bxi, byi, vl[s]), b = label_global(g, nbx, nby, vl[nb]);
         if (a != b)
-            link = guf_union_pair(labels, a, b, fault);
+            link = guf_union_pair(labels, a, b, g.L0 * g.L1, fault);
     }
     if (linked)
         linked[((size_t)byi * g.nbx + bxi) * (g.BX + g.BY) + t] = link;
@@ -1085,7 +1085,7 @@ __device__ __forceinline__ void resolve_block(const Geo &g, const uint32_t bxi, 
 {
     const uint32_t b = linked[((size_t)byi * g.nbx + bxi) * (g.BX + g.BY) + t];
     if (b != kNoLink)
-        labels[b] = guf_find(labels, b, fault);  // the tree's minimum: other finds' atomicMin never undo it
+        labels[b] = guf_find(labels, b, g.L0 * g.L1, fault);  // the tree's minimum: other finds' atomicMin never undo it
 }
 
 // Shared memory of flip_block: the resolved label of every block root.
@@ -1138,7 +1138,7 @@ __device__ __forceinline__ void flip_block(const Geo &g, const uint32_t bxi, con
 #pragma unroll
                 for (int j = 0; j < 4; ++j)
                     if (!(v[j] & kLocalFlag))  // a block root: v is its parent (itself unless merged)
-                        res[l + j] = kResolved || v[j] == s + j ? v[j] : guf_find(labels, v[j], fault);
+                        res[l + j] = kResolved || v[j] == s + j ? v[j] : guf_find(labels, v[j], L0 * g.L1, fault);
             }
         }
         __syncthreads();
@@ -1166,7 +1166,7 @@ __device__ __forceinline__ void flip_block(const Geo &g, const uint32_t bxi, con
             const uint32_t site = base + yl * L0 + xl;
             const uint32_t v = labels[site];
             if (!(v & kLocalFlag))
-                res[yl * BX + xl] = kResolved || v == site ? v : guf_find(labels, v, fault);
+                res[yl * BX + xl] = kResolved || v == site ? v : guf_find(labels, v, L0 * g.L1, fault);
         }
     __syncthreads();
     if ((L0 & 3u) == 0) {

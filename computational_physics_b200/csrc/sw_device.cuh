@@ -148,20 +148,32 @@ __device__ __forceinline__ void uf_union(uint32_t *p, uint32_t a, uint32_t b)
 // the path as they go (x's parent becomes its grandparent); the update is an atomicMin, which
 // only ever moves a pointer to an ancestor, so it is safe against concurrent unions and keeps
 // the trees shallow.  Every loop is capped: parents strictly decrease, so a chain longer than
-// kChainCap means corrupt labels; the walk then stops and raises *fault.
+// kChainCap means corrupt labels; the walk then stops and raises *fault.  Every value read is
+// checked against the site count before it is used as an index: a label outside the lattice
+// (only corrupt labels hold one) stops the walk too.  Fault bits: 1 chain cap, 2 union retry
+// cap, 4 label outside the lattice.
 constexpr uint32_t kChainCap = 1u << 22;
 constexpr uint32_t kUnionRetryCap = 1u << 16;
+constexpr unsigned int kFaultChain = 1u, kFaultRetry = 2u, kFaultRange = 4u;
 
-__device__ __forceinline__ uint32_t guf_find(uint32_t *p, uint32_t x, unsigned int *fault)
+__device__ __forceinline__ uint32_t guf_find(uint32_t *p, uint32_t x, const uint32_t n_sites, unsigned int *fault)
 {
+    if (x >= n_sites) {
+        atomicOr(fault, kFaultRange);
+        return 0;
+    }
     const volatile uint32_t *vp = p;
     uint32_t y = vp[x];
     for (uint32_t n = 0; y != x; ++n) {
+        if (y >= n_sites || n >= kChainCap) {
+            atomicOr(fault, y >= n_sites ? kFaultRange : kFaultChain);
+            return x;
+        }
         const uint32_t z = vp[y];
         if (z == y)
             return y;
-        if (n >= kChainCap) {
-            atomicOr(fault, 1u);
+        if (z >= n_sites) {
+            atomicOr(fault, kFaultRange);
             return y;
         }
         atomicMin(p + x, z);  // path halving
@@ -171,26 +183,6 @@ __device__ __forceinline__ uint32_t guf_find(uint32_t *p, uint32_t x, unsigned i
     return x;
 }
 
-__device__ __forceinline__ void guf_union(uint32_t *p, uint32_t a, uint32_t b, unsigned int *fault)
-{
-    for (uint32_t n = 0; n < kUnionRetryCap; ++n) {
-        a = guf_find(p, a, fault);
-        b = guf_find(p, b, fault);
-        if (a == b)
-            return;
-        if (a > b) {
-            const uint32_t t = a;
-            a = b;
-            b = t;
-        }
-        const uint32_t old = atomicMin(p + b, a);
-        if (old == b)
-            return;
-        b = old;
-    }
-    atomicOr(fault, 2u);
-}
-
 constexpr uint32_t kNoLink = 0xFFFFFFFFu;  // guf_union_pair linked no root
 
 // The same union with the two root walks advancing together, one level per step, so the loads
@@ -198,18 +190,27 @@ constexpr uint32_t kNoLink = 0xFFFFFFFFu;  // guf_union_pair linked no root
 // grandparent (path splitting, by atomicMin as above).  Same caps and fault bits.  Returns the
 // root it linked below the other (each root is linked at most once: afterwards it is no root),
 // or kNoLink when the two were already one tree.
-__device__ __forceinline__ uint32_t guf_union_pair(uint32_t *p, uint32_t a, uint32_t b, unsigned int *fault)
+__device__ __forceinline__ uint32_t guf_union_pair(uint32_t *p, uint32_t a, uint32_t b, const uint32_t n_sites,
+                                                   unsigned int *fault)
 {
     const volatile uint32_t *vp = p;
     for (uint32_t n = 0; n < kUnionRetryCap; ++n) {
+        if (a >= n_sites || b >= n_sites) {  // the arguments, or a parent read by a failed link
+            atomicOr(fault, kFaultRange);
+            return kNoLink;
+        }
         uint32_t ya = vp[a], yb = vp[b];
         for (uint32_t k = 0; ya != a || yb != b; ++k) {
-            if (k >= kChainCap) {
-                atomicOr(fault, 1u);
+            if (k >= kChainCap || ya >= n_sites || yb >= n_sites) {
+                atomicOr(fault, k >= kChainCap ? kFaultChain : kFaultRange);
                 return kNoLink;
             }
             const uint32_t za = ya != a ? vp[ya] : ya;
             const uint32_t zb = yb != b ? vp[yb] : yb;
+            if (za >= n_sites || zb >= n_sites) {
+                atomicOr(fault, kFaultRange);
+                return kNoLink;
+            }
             if (ya != a) {
                 if (za != ya)
                     atomicMin(p + a, za);
@@ -235,7 +236,7 @@ __device__ __forceinline__ uint32_t guf_union_pair(uint32_t *p, uint32_t a, uint
             return b;
         b = old;
     }
-    atomicOr(fault, 2u);
+    atomicOr(fault, kFaultRetry);
     return kNoLink;
 }
 

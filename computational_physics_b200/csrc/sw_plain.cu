@@ -341,7 +341,7 @@ int check_fault(swb_lattice *h)
     SWB_CUDA(cudaMemcpyAsync(&f, h->fault, sizeof(f), cudaMemcpyDeviceToHost, h->stream));
     SWB_CUDA(cudaStreamSynchronize(h->stream));
     if (f)
-        return fail(SWB_ERR_STATE, "label chase exceeded %u steps (fault word %u)", kChainCap, f);
+        return fail(SWB_ERR_STATE, "label union-find fault (word %u: 1 chain over %u steps, 2 union retries, 4 label outside the lattice)", f, kChainCap);
     return SWB_OK;
 }
 
@@ -1081,7 +1081,7 @@ int swb_sweep_static(void *stream, uint32_t L0, uint32_t L1, uint32_t tile_x, ui
         SWB_CUDA(cudaMemcpyAsync(&f, h.fault, sizeof(f), cudaMemcpyDeviceToHost, h.stream));
         SWB_CUDA(cudaStreamSynchronize(h.stream));
         if (f)
-            return fail(SWB_ERR_STATE, "label chase exceeded %u steps (fault word %u)", kChainCap, f);
+            return fail(SWB_ERR_STATE, "label union-find fault (word %u: 1 chain over %u steps, 2 union retries, 4 label outside the lattice)", f, kChainCap);
     }
     return SWB_OK;
 }

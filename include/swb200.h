@@ -263,7 +263,7 @@ int swb_update_host(swb_lattice *h, float temperature, const uint8_t *spins_in, 
  * resolved by the flip itself (the three-kernel form of swb_sweep; at 2048 x 2048 about 5 %
  * slower than the four-kernel form swb_sweep uses there): the array has no room for the merge
  * slots.  Asynchronous on `stream` (NULL = default stream); with wait != 0 the call
- * synchronises the stream and reports a label-chase fault as SWB_ERR_STATE.  With wait == 0 such
+ * synchronises the stream and reports a label union-find fault as SWB_ERR_STATE.  With wait == 0 such
  * a fault is not reported: the next call clears the fault word. */
 int swb_sweep_static(void *stream, uint32_t L0, uint32_t L1, uint32_t tile_x, uint32_t tile_y, uint32_t lcg_width,
                      float temperature, uint32_t n_sweeps, uint8_t *spins, uint32_t *rng_state, uint8_t *rng_sel,
