@@ -1004,8 +1004,10 @@ __device__ __forceinline__ void assign_block(const Geo &g, const uint32_t bxi, c
 
 // assign_block with the tile shape as compile-time constants for the common shapes (lcg width
 // 16), the runtime form otherwise; full 128 x 32 blocks of 16 x 8 tiles take the fixed-shape
-// scanline.
-template <int W>
+// scanline.  kAllShapes false keeps only 16 x 8 and 16 x 4 (the tiles the B200 table picks):
+// every compile-time shape in the kernel costs the 16 x 8 path registers and instruction
+// fetches (the 512-lattice mix's assign: 0.271 ms with all seven shapes, 0.245 ms with two).
+template <int W, bool kAllShapes = true>
 __device__ __forceinline__ void assign_block_any(const Geo &g, const uint32_t bxi, const uint32_t byi,
                                                  const uint8_t *__restrict__ spins, uint32_t *__restrict__ labels,
                                                  uint32_t *__restrict__ rng_state, uint8_t *__restrict__ rng_sel,
@@ -1021,12 +1023,14 @@ __device__ __forceinline__ void assign_block_any(const Geo &g, const uint32_t bx
     }
     if constexpr (W == 16) {
         SWB_TILE(16, 8)
-        SWB_TILE(8, 8)
-        SWB_TILE(32, 4)
-        SWB_TILE(16, 16)
-        SWB_TILE(8, 16)
-        SWB_TILE(32, 8)
         SWB_TILE(16, 4)
+        if constexpr (kAllShapes) {
+            SWB_TILE(8, 8)
+            SWB_TILE(32, 4)
+            SWB_TILE(16, 16)
+            SWB_TILE(8, 16)
+            SWB_TILE(32, 8)
+        }
     }
 #undef SWB_TILE
     assign_block<W, 0, 0, false, false>(g, bxi, byi, spins, labels, rng_state, rng_sel, rng_iter, thr, edge,
@@ -1037,9 +1041,11 @@ __device__ __forceinline__ void assign_block_any(const Geo &g, const uint32_t bx
 // row t of the right edge, BY <= t < BY + BX column t - BY of the bottom edge.  With `linked`,
 // slot t of the block's BX + BY slots receives the root this thread's union linked (kNoLink
 // for none): every block root the merge turns into a non-root appears in exactly one slot.
+// With active false (a lattice whose sweep budget is spent) nothing is written; the edge words
+// are read all the same, so their load need not wait for the budget's.
 __device__ __forceinline__ void merge_block(const Geo &g, const uint32_t bxi, const uint32_t byi, const uint32_t t,
                                             const uint32_t *__restrict__ edge, uint32_t *labels, unsigned int *fault,
-                                            uint32_t *__restrict__ linked)
+                                            uint32_t *__restrict__ linked, const bool active = true)
 {
     const uint32_t x0 = bxi * g.BX, y0 = byi * g.BY;
     const uint32_t bxv = min(g.BX, g.L0 - x0), byv = min(g.BY, g.L1 - y0);
@@ -1064,13 +1070,13 @@ __device__ __forceinline__ void merge_block(const Geo &g, const uint32_t bxi, co
         }
     }
     uint32_t link = kNoLink;
-    if (go) {
+    if (go && active) {
         const volatile uint32_t *vl = labels;
         const uint32_t a = label_global(g, bxi, byi, vl[s]), b = label_global(g, nbx, nby, vl[nb]);
         if (a != b)
             link = guf_union_pair(labels, a, b, g.L0 * g.L1, fault);
     }
-    if (linked)
+    if (linked && active)
         linked[((size_t)byi * g.nbx + bxi) * (g.BX + g.BY) + t] = link;
 }
 
@@ -1081,10 +1087,10 @@ __device__ __forceinline__ void merge_block(const Geo &g, const uint32_t bxi, co
 // CTA's barrier.
 __device__ __forceinline__ void resolve_block(const Geo &g, const uint32_t bxi, const uint32_t byi, const uint32_t t,
                                               const uint32_t *__restrict__ linked, uint32_t *labels,
-                                              unsigned int *fault)
+                                              unsigned int *fault, const bool active = true)
 {
     const uint32_t b = linked[((size_t)byi * g.nbx + bxi) * (g.BX + g.BY) + t];
-    if (b != kNoLink)
+    if (b != kNoLink && active)
         labels[b] = guf_find(labels, b, g.L0 * g.L1, fault);  // the tree's minimum: other finds' atomicMin never undo it
 }
 
@@ -1099,9 +1105,12 @@ __host__ __device__ inline uint32_t flip_smem_bytes(const Geo &g)
 // blocks) into shared memory, or with kResolved (resolve_block ran) take their label as it is;
 // every site then reads its root's result there and flips iff the cluster's label is odd.
 // kWriteLabels stores the resolved global labels (the reference's ResolveLabels output).
+// With active false (a lattice whose sweep budget is spent) the block is read but nothing is
+// written, so the loads need not wait for the budget's.
 template <bool kWriteLabels, int kQuads = 2, bool kResolved = false>
 __device__ __forceinline__ void flip_block(const Geo &g, const uint32_t bxi, const uint32_t byi, uint8_t *spins,
-                                           uint32_t *labels, unsigned int *fault, unsigned char *smem)
+                                           uint32_t *labels, unsigned int *fault, unsigned char *smem,
+                                           const bool active = true)
 {
     const uint32_t BX = g.BX, L0 = g.L0;
     uint32_t *res = reinterpret_cast<uint32_t *>(smem);
@@ -1138,10 +1147,13 @@ __device__ __forceinline__ void flip_block(const Geo &g, const uint32_t bxi, con
 #pragma unroll
                 for (int j = 0; j < 4; ++j)
                     if (!(v[j] & kLocalFlag))  // a block root: v is its parent (itself unless merged)
-                        res[l + j] = kResolved || v[j] == s + j ? v[j] : guf_find(labels, v[j], L0 * g.L1, fault);
+                        res[l + j] = kResolved || !active || v[j] == s + j ? v[j]
+                                                                            : guf_find(labels, v[j], L0 * g.L1, fault);
             }
         }
         __syncthreads();
+        if (!active)
+            return;
 #pragma unroll
         for (int k = 0; k < kQuads; ++k) {
             const uint32_t yl = yl0 + k * rstep;
@@ -1166,9 +1178,11 @@ __device__ __forceinline__ void flip_block(const Geo &g, const uint32_t bxi, con
             const uint32_t site = base + yl * L0 + xl;
             const uint32_t v = labels[site];
             if (!(v & kLocalFlag))
-                res[yl * BX + xl] = kResolved || v == site ? v : guf_find(labels, v, L0 * g.L1, fault);
+                res[yl * BX + xl] = kResolved || !active || v == site ? v : guf_find(labels, v, L0 * g.L1, fault);
         }
     __syncthreads();
+    if (!active)
+        return;
     if ((L0 & 3u) == 0) {
         for (uint32_t yl = warp; yl < byv; yl += nwarps) {
             const uint32_t row = base + yl * L0;

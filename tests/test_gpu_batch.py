@@ -19,6 +19,17 @@ MIX = [
     (512, 512, (16, 8), 2.3, 13, (0, 0)),
 ]
 
+# Only the tiles the lean batched assign instance compiles (16 x 8 and 16 x 4) or neither
+# instance does (16 x 2, the runtime path): the engine launches the lean instance.
+LEAN_MIX = [
+    (64, 64, (16, 4), 2.2691853, 21, (0, 0)),
+    (96, 96, (16, 8), 2.1, 22, (0, 0)),
+    (128, 128, (16, 8), 2.5, 23, (4, 2)),
+    (100, 38, (16, 8), 3.0, 24, (0, 0)),     # ragged tiles
+    (64, 32, (16, 2), 2.4, 25, (0, 0)),
+    (384, 384, (16, 8), 2.3, 26, (0, 0)),
+]
+
 
 def _oracle_run(oracle, spins, tile, T, seed, sweeps, W=16):
     L1, L0 = spins.shape
@@ -29,11 +40,12 @@ def _oracle_run(oracle, spins, tile, T, seed, sweeps, W=16):
     return s, rng
 
 
-def test_mix_bit_exact(gpu, oracle):
+@pytest.mark.parametrize("mix", [MIX, LEAN_MIX], ids=["all_shapes", "lean"])
+def test_mix_bit_exact(gpu, oracle, mix):
     rounds = 6
     with gpu.BatchedSW(capacity=64) as b:
         ids, starts = [], []
-        for k, (L0, L1, tile, T, seed, block) in enumerate(MIX):
+        for k, (L0, L1, tile, T, seed, block) in enumerate(mix):
             i = b.add(L0, L1, T, seed, tile, block)
             start = oracle.hot_start(L0, L1, 1) if k % 2 == 0 else \
                 np.random.default_rng(k).integers(0, 2, (L1, L0), dtype=np.uint8)
@@ -42,7 +54,7 @@ def test_mix_bit_exact(gpu, oracle):
             starts.append(start)
         b.sweep(rounds)
         b.synchronize()
-        for i, start, (L0, L1, tile, T, seed, block) in zip(ids, starts, MIX):
+        for i, start, (L0, L1, tile, T, seed, block) in zip(ids, starts, mix):
             want, rng = _oracle_run(oracle, start, tile, T, seed, rounds)
             assert np.array_equal(b.get_spins(i), want), (L0, L1, tile)
             st, a, c, it = b.get_rng(i)
