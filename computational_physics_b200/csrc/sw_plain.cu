@@ -74,7 +74,7 @@ constexpr uint32_t kAssignThreads = 512;  // at most this many lcg lanes per blo
 // (the tile-local stage only through the runtime-shape instance, which labels tile by tile).
 // kMeasure: the instance that also measures the spins it starts from (`meas`), used by the
 // sweep after a measured one; a separate instance so the others carry none of its registers.
-template <int W, int TXc, int TYc, bool kMeasure>
+template <int W, int TXc, int TYc, bool kMeasure, bool kFixedOnly = false>
 __global__ void __launch_bounds__(kAssignThreads, 4) k_assign(const Geo g, const uint8_t *__restrict__ spins,
                                                  uint32_t *__restrict__ labels, uint32_t *__restrict__ rng_state,
                                                  uint8_t *__restrict__ rng_sel, uint32_t *__restrict__ rng_iter,
@@ -82,8 +82,9 @@ __global__ void __launch_bounds__(kAssignThreads, 4) k_assign(const Geo g, const
                                                  const MeasureArgs meas)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    assign_block<W, TXc, TYc, false, true, true>(g, blockIdx.x, blockIdx.y, spins, labels, rng_state, rng_sel,
-                                                 rng_iter, thr, edge, dump, kMeasure ? meas : MeasureArgs{}, smem);
+    assign_block<W, TXc, TYc, false, true, true, kFixedOnly>(g, blockIdx.x, blockIdx.y, spins, labels, rng_state,
+                                                             rng_sel, rng_iter, thr, edge, dump,
+                                                             kMeasure ? meas : MeasureArgs{}, smem);
 }
 
 __global__ void __launch_bounds__(256) k_merge(const Geo g, const uint32_t *__restrict__ edge, uint32_t *labels,
@@ -228,6 +229,21 @@ int launch_assign_k(swb_lattice *h, float p_add, const AssignDump &dump, const M
     const Geo &g = h->g;
     // Whole warps: the draws use full-warp shuffles and ballots; surplus lanes have no tile.
     const dim3 grid(g.nbx, g.nby), block((g.TBX * g.TBY * W + 31) / 32 * 32);
+    if constexpr (W == 16 && TXc == 16 && TYc == 8) {
+        // every block a full 128 x 32 block of 512 threads: the fixed-only instance
+        if (g.BX == 128 && g.BY == 32 && g.L0 % 128 == 0 && g.L1 % 32 == 0 && block.x == 512) {
+            if (meas.obs)
+                k_assign<W, TXc, TYc, true, true><<<grid, block, h->smem_assign, h->stream>>>(
+                    g, h->spins, h->labels, h->rng_state, h->rng_sel, h->rng_iter, accept_threshold(p_add), h->edge,
+                    dump, meas);
+            else
+                k_assign<W, TXc, TYc, false, true><<<grid, block, h->smem_assign, h->stream>>>(
+                    g, h->spins, h->labels, h->rng_state, h->rng_sel, h->rng_iter, accept_threshold(p_add), h->edge,
+                    dump, meas);
+            SWB_LAUNCHED();
+            return SWB_OK;
+        }
+    }
     if (meas.obs)
         k_assign<W, TXc, TYc, true><<<grid, block, h->smem_assign, h->stream>>>(
             g, h->spins, h->labels, h->rng_state, h->rng_sel, h->rng_iter, accept_threshold(p_add), h->edge, dump, meas);
