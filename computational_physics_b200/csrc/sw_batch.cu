@@ -155,10 +155,15 @@ __global__ void __launch_bounds__(kFlipThreads, 6) kb_flip(const BatchLat *lats,
     extern __shared__ __align__(16) unsigned char smem[];
     for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
         const BlockRec r = recs[item];
-        const bool active = lats[r.lat].sweeps_left != 0;
-        flip_block<false, 4, true>(rec_geo(r), r.bxy & 0xFFFFu, r.bxy >> 16, r.spins, r.labels, fault, smem, active);
-        if (item + gridDim.x < total)
-            __syncthreads();  // the next item reuses the shared memory
+        // A lattice whose budget is spent stays in the lists until the host removes it (a
+        // server keeps finished jobs until it needs their memory): its blocks load nothing.
+        // Loading them anyway and only skipping the stores, which frees the loads from the
+        // budget's, made the mix 1 % faster and served jobs 23 % slower.
+        if (lats[r.lat].sweeps_left != 0) {
+            flip_block<false, 4, true>(rec_geo(r), r.bxy & 0xFFFFu, r.bxy >> 16, r.spins, r.labels, fault, smem);
+            if (item + gridDim.x < total)
+                __syncthreads();  // the next item reuses the shared memory
+        }
     }
 }
 

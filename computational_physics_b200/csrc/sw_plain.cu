@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(kAssignThreads, 4) k_assign(const Geo g, const
                                                  const MeasureArgs meas)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    assign_block<W, TXc, TYc, false, true, true, kFixedOnly>(g, blockIdx.x, blockIdx.y, spins, labels, rng_state,
+    assign_block<W, TXc, TYc, kFixedOnly, true, true, kFixedOnly>(g, blockIdx.x, blockIdx.y, spins, labels, rng_state,
                                                              rng_sel, rng_iter, thr, edge, dump,
                                                              kMeasure ? meas : MeasureArgs{}, smem);
 }
