@@ -106,14 +106,26 @@ __device__ __forceinline__ uint32_t label_global3(const Geo3 &g, uint32_t bxi, u
     return ((bzi * g.BZ + zl) * g.L1 + byi * g.BY + yl) * g.L0 + bxi * g.BX + xl;
 }
 
-template <int W>
-__global__ void __launch_bounds__(k3Threads) k3_assign(const Geo3 g, const uint8_t *__restrict__ spins,
+// kFixed: tile 16 x 4 x 4, lcg width 16, and every block a full 32 x 8 x 8 block (the caller
+// checked): the block and tile shape are constants, so the site index arithmetic is shifts and
+// the loops have fixed trip counts.
+template <int W, bool kFixed = false>
+__global__ void __launch_bounds__(k3Threads) k3_assign(const Geo3 g_in, const uint8_t *__restrict__ spins,
                                                         uint32_t *__restrict__ labels, uint32_t *__restrict__ rng_state,
                                                         uint8_t *__restrict__ rng_sel, uint32_t *__restrict__ rng_iter,
                                                         const uint32_t thr, uint32_t *__restrict__ faces,
                                                         uint8_t *__restrict__ dump_bonds)
 {
     extern __shared__ __align__(16) unsigned char smem[];
+    static_assert(!kFixed || W == 16, "the fixed form is lcg width 16");
+    Geo3 gfix = g_in;
+    if constexpr (kFixed) {
+        gfix.TX = 16; gfix.TY = 4; gfix.TZ = 4;
+        gfix.TBX = 2; gfix.TBY = 2; gfix.TBZ = 2;
+        gfix.BX = 32; gfix.BY = 8; gfix.BZ = 8;
+        gfix.wx = 2; gfix.wy = 8; gfix.wz = 8;
+    }
+    const Geo3 &g = kFixed ? gfix : g_in;
     const Assign3Smem S = assign3_smem(g);
     uint32_t *parent = reinterpret_cast<uint32_t *>(smem + S.parent);
     uint8_t *acc = smem + S.acc, *box = smem + S.box;
@@ -121,8 +133,9 @@ __global__ void __launch_bounds__(k3Threads) k3_assign(const Geo3 g, const uint8
     const uint32_t bxi = blockIdx.x, byi = blockIdx.y, bzi = blockIdx.z;
     const uint32_t BX = g.BX, BY = g.BY, BZ = g.BZ, NS = BX * BY * BZ;
     const uint32_t x0 = bxi * BX, y0 = byi * BY, z0 = bzi * BZ;
-    const uint32_t bxv = min(BX, g.L0 - x0), byv = min(BY, g.L1 - y0), bzv = min(BZ, g.L2 - z0);
-    const uint32_t tid = threadIdx.x, nthr = blockDim.x;
+    const uint32_t bxv = kFixed ? BX : min(BX, g.L0 - x0), byv = kFixed ? BY : min(BY, g.L1 - y0);
+    const uint32_t bzv = kFixed ? BZ : min(BZ, g.L2 - z0);
+    const uint32_t tid = threadIdx.x, nthr = kFixed ? k3Threads : blockDim.x;
     const size_t plane = (size_t)g.L0 * g.L1;
 
     for (uint32_t l = tid; l < NS; l += nthr) {
@@ -154,8 +167,9 @@ __global__ void __launch_bounds__(k3Threads) k3_assign(const Geo3 g, const uint8
         const uint32_t tgx = bxi * g.TBX + tbx, tgy = byi * g.TBY + tby, tgz = bzi * g.TBZ + tbz;
         const bool on = tb < ntb && tgx < g.n0 && tgy < g.n1 && tgz < g.n2 && tid < ((ntb * W + 31) & ~31u);
         const uint32_t tile = (tgz * g.n1 + tgy) * g.n0 + tgx;
-        const uint32_t iimax = on ? min(TX, g.L0 - tgx * TX) : 0, jjmax = on ? min(TY, g.L1 - tgy * TY) : 0;
-        const uint32_t kkmax = on ? min(TZ, g.L2 - tgz * TZ) : 0;
+        const uint32_t iimax = on ? (kFixed ? TX : min(TX, g.L0 - tgx * TX)) : 0;
+        const uint32_t jjmax = on ? (kFixed ? TY : min(TY, g.L1 - tgy * TY)) : 0;
+        const uint32_t kkmax = on ? (kFixed ? TZ : min(TZ, g.L2 - tgz * TZ)) : 0;
         const uint32_t ox = tbx * TX, oy = tby * TY, oz = tbz * TZ;  // the tile's origin in the block
         uint32_t st = 0, sel = 0, it = 0;
         if (on) {
@@ -474,6 +488,13 @@ int launch_sweep3(swb_lattice3 *h, float temperature, uint8_t *dump_bonds, bool 
     const Geo3 &g = h->g;
     const dim3 grid(g.nbx, g.nby, g.nbz);
     const uint32_t thr = accept_threshold(swb_p_add(temperature));
+    const bool fixed = h->W == 16 && g.TX == 16 && g.TY == 4 && g.TZ == 4 && g.BX == 32 && g.BY == 8 && g.BZ == 8 &&
+                       g.L0 % 32 == 0 && g.L1 % 8 == 0 && g.L2 % 8 == 0;
+    if (fixed)
+        k3_assign<16, true><<<grid, k3Threads, h->smem_assign, h->stream>>>(g, h->spins, h->labels, h->rng_state,
+                                                                            h->rng_sel, h->rng_iter, thr, h->faces,
+                                                                            dump_bonds);
+    else
     switch (h->W) {
     case 8: k3_assign<8><<<grid, k3Threads, h->smem_assign, h->stream>>>(g, h->spins, h->labels, h->rng_state, h->rng_sel, h->rng_iter, thr, h->faces, dump_bonds); break;
     case 16: k3_assign<16><<<grid, k3Threads, h->smem_assign, h->stream>>>(g, h->spins, h->labels, h->rng_state, h->rng_sel, h->rng_iter, thr, h->faces, dump_bonds); break;
