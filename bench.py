@@ -257,12 +257,12 @@ def assign_bytes(n_sites: int, n_tiles: int, W: int) -> float:
 
 # DRAM traffic of one assign pass over a workload (dram__bytes_read.sum + dram__bytes_write.sum)
 # from one ncu capture of the same kernel, per site: the batched mix of 512 lattices (39,603,200
-# sites; the round runs its two lattice groups as two launches: 33,117,952 + 33,138,688 B read,
-# 35,994,112 + 37,903,616 B written) and one 8192 x 8192 lattice, tile 16 x 8 (111,203,584 B read
-# + 253,751,552 B written).  Traffic grows with the sites swept, so other sizes scale by their
+# sites; the round runs its two lattice groups as two launches: 33,116,672 + 33,139,200 B read,
+# 36,331,520 + 38,318,336 B written) and one 8192 x 8192 lattice, tile 16 x 8 (111,228,928 B read
+# + 253,859,584 B written).  Traffic grows with the sites swept, so other sizes scale by their
 # site count.
-ASSIGN_TRAFFIC_PER_SITE = {"kb_assign": (33_117_952 + 33_138_688 + 35_994_112 + 37_903_616) / 39_603_200,
-                           "k_assign": (111_203_584 + 253_751_552) / 8192 ** 2}
+ASSIGN_TRAFFIC_PER_SITE = {"kb_assign": (33_116_672 + 33_139_200 + 36_331_520 + 38_318_336) / 39_603_200,
+                           "k_assign": (111_228_928 + 253_859_584) / 8192 ** 2}
 
 
 def flip_bytes(n_sites: int) -> float:
