@@ -223,6 +223,41 @@ def test_host_io_steps(gpu, oracle):
         assert np.array_equal(b.get_spins(extra), want_x)
 
 
+def test_assign_instance_follows_the_lattice_set(gpu, oracle):
+    """A batch of 16 x 8 / 16 x 4 lattices runs the lean assign instance; adding an 8 x 8 lattice
+    switches the round to the all-shapes instance and removing it switches back, and every
+    lattice stays on the oracle's sweeps through both changes."""
+    shapes = [(128, 64, (16, 8), 2.3, 31), (64, 64, (16, 4), 2.5, 32)]
+    with gpu.BatchedSW(capacity=4) as b:
+        ids, state = [], []
+        for L0, L1, tile, T, seed in shapes:
+            i = b.add(L0, L1, T, seed, tile)
+            s0 = oracle.hot_start(L0, L1, seed)
+            b.set_spins(i, s0)
+            ids.append(i)
+            state.append([s0.copy(), oracle.rng_init(16, num_tiles(L0, L1, *tile), seed), tile, T])
+
+        def advance(n):
+            for st in state:
+                for _ in range(n):
+                    oracle.sweep(st[0], st[2][0], st[2][1], st[1], T=st[3])
+
+        b.sweep(2)
+        advance(2)
+        extra = b.add(96, 64, 2.2, 33, (8, 8))
+        x0 = oracle.hot_start(96, 64, 33)
+        b.set_spins(extra, x0)
+        b.sweep(3)
+        advance(3)
+        want_x, _ = _oracle_run(oracle, x0, (8, 8), 2.2, 33, 3)
+        assert np.array_equal(b.get_spins(extra), want_x)
+        b.remove(extra)
+        b.sweep(2)
+        advance(2)
+        for i, st in zip(ids, state):
+            assert np.array_equal(b.get_spins(i), st[0])
+
+
 @pytest.mark.parametrize("rounds", [1, 2, 5])
 def test_host_io_rounds(gpu, oracle, rounds):
     """update_host_io_rounds: the pipelined rounds through the two HostIO arenas give the
