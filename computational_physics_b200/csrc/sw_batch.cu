@@ -155,15 +155,13 @@ __global__ void __launch_bounds__(kFlipThreads, 6) kb_flip(const BatchLat *lats,
     extern __shared__ __align__(16) unsigned char smem[];
     for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
         const BlockRec r = recs[item];
-        // A lattice whose budget is spent stays in the lists until the host removes it (a
-        // server keeps finished jobs until it needs their memory): its blocks load nothing.
-        // Loading them anyway and only skipping the stores, which frees the loads from the
-        // budget's, made the mix 1 % faster and served jobs 23 % slower.
-        if (lats[r.lat].sweeps_left != 0) {
-            flip_block<false, 4, true>(rec_geo(r), r.bxy & 0xFFFFu, r.bxy >> 16, r.spins, r.labels, fault, smem);
-            if (item + gridDim.x < total)
-                __syncthreads();  // the next item reuses the shared memory
-        }
+        // The budget is read beside the data, not ahead of it: a lattice whose budget ran out
+        // leaves the lists at the engine's next call, so only the rest of the call in which it
+        // finished reads (and does not write) its blocks.
+        const bool active = lats[r.lat].sweeps_left != 0;
+        flip_block<false, 4, true>(rec_geo(r), r.bxy & 0xFFFFu, r.bxy >> 16, r.spins, r.labels, fault, smem, active);
+        if (item + gridDim.x < total)
+            __syncthreads();  // the next item reuses the shared memory
     }
 }
 
@@ -319,6 +317,7 @@ struct HostLat {
     BatchLat d{};             // host copy of the descriptor
     uint64_t bytes = 0;       // device bytes held
     void *mem = nullptr;      // one allocation for all buffers of the lattice
+    uint64_t sched_round = 0; // the engine's round count when d.sweeps_left was last set
 };
 
 }  // namespace
@@ -365,6 +364,7 @@ struct swb_batch {
     std::vector<cudaEvent_t> marks;         // swb_batch_mark's events, a ring
     uint32_t next_mark = 0;
     bool lists_dirty = true;
+    uint64_t round_count = 0;  // rounds queued so far (every listed lattice with budget left sweeps once)
     bool assign_all_shapes = true;  // an active lattice has a tile only the all-shapes assign compiles
     int grid_measure = 0;
     uint32_t smem_assign = 0, smem_flip = 0;
@@ -432,13 +432,25 @@ std::vector<BlockRec> make_recs(const swb_batch *b, const std::vector<uint2> &it
     return recs;
 }
 
+// A lattice whose budget the queued rounds have used up (known on the host: every round
+// sweeps every listed lattice with budget left once).  It leaves the lists at their next
+// rebuild, so rounds launch nothing for it; a server keeps finished jobs until it needs their
+// memory.
+bool budget_spent(const swb_batch *b, const HostLat &h)
+{
+    return h.d.sweeps_left != kUnlimited && b->round_count - h.sched_round >= h.d.sweeps_left;
+}
+
 int rebuild_lists(swb_batch *b)
 {
+    for (uint32_t id : b->active)
+        if (budget_spent(b, b->lats[id]))
+            b->lists_dirty = true;
     if (!b->lists_dirty)
         return SWB_OK;
     b->active.clear();
     for (uint32_t i = 0; i < b->capacity; ++i)
-        if (b->lats[i].used)
+        if (b->lats[i].used && !budget_spent(b, b->lats[i]))
             b->active.push_back(i);
     // big lattices first: their many items start early and balance the tail
     std::stable_sort(b->active.begin(), b->active.end(), [&](uint32_t x, uint32_t y) {
@@ -688,6 +700,7 @@ int rounds(swb_batch *b, uint32_t n_rounds, bool any_measure)
     for (uint32_t r = 0; r < n_rounds; ++r) {
         SWB_CUDA(cudaGraphLaunch(ge, b->stream));
         g_launches.fetch_add(round_launches(b, any_measure), std::memory_order_relaxed);
+        b->round_count += 1;
     }
     return SWB_OK;
 }
@@ -957,8 +970,12 @@ int swb_batch_set_schedule(swb_batch *b, uint32_t id, uint32_t sweeps, uint32_t 
     SWB_CUDA(cudaMemcpyAsync(&b->d_lats[id].sweeps_left, &v[0], 4, cudaMemcpyHostToDevice, b->stream));
     SWB_CUDA(cudaMemcpyAsync(&b->d_lats[id].measure_every, &v[1], 4, cudaMemcpyHostToDevice, b->stream));
     SWB_CUDA(cudaStreamSynchronize(b->stream));
+    const bool was_spent = budget_spent(b, *h);
     h->d.sweeps_left = sweeps;
     h->d.measure_every = measure_every;
+    h->sched_round = b->round_count;
+    if (budget_spent(b, *h) != was_spent)  // joins or leaves the lists
+        b->lists_dirty = true;
     return SWB_OK;
 }
 
@@ -1094,6 +1111,7 @@ int swb_batch_sweep_timed(swb_batch *b, uint32_t n_rounds, int per_kernel, float
             SWB_CUDA(cudaEventRecord(ev[4], b->stream));
             if ((rc = launch_end_round(b, b->stream, false)))
                 break;
+            b->round_count += 1;
             SWB_CUDA(cudaEventSynchronize(ev[4]));
             float t;
             SWB_CUDA(cudaEventElapsedTime(&t, ev[1], ev[2]));
@@ -1408,9 +1426,11 @@ int update_host_rounds(swb_batch *b, uint32_t count, const uint32_t *ids, const 
                     return rc;
                 kb_stage_copy<<<sgrid, 256, 0, b->stream>>>(b->d_copies + gs[g], b->d_stage, 0);
                 SWB_LAUNCHED();
-                if (g + 1 == G)  // every listed and unlisted lattice has swept: close the round
+                if (g + 1 == G) {  // every listed and unlisted lattice has swept: close the round
                     if (int rc = launch_end_round(b, b->stream, false))
                         return rc;
+                    b->round_count += 1;
+                }
                 SWB_CUDA(cudaEventRecord(ev[G + g], b->stream));
                 SWB_CUDA(cudaStreamWaitEvent(b->s_out, ev[G + g], 0));
                 for (uint32_t k = gs[g]; k < gs[g + 1];) {
