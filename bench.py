@@ -257,11 +257,11 @@ def assign_bytes(n_sites: int, n_tiles: int, W: int) -> float:
 
 # DRAM traffic of one assign pass over a workload (dram__bytes_read.sum + dram__bytes_write.sum)
 # from one ncu capture of the same kernel, per site: the batched mix of 512 lattices (39,603,200
-# sites; the round runs its two lattice groups as two launches: 33,116,672 + 33,139,200 B read,
-# 36,331,520 + 38,318,336 B written) and one 8192 x 8192 lattice, tile 16 x 8 (111,228,928 B read
+# sites; the round runs its two lattice groups as two launches: 33,125,632 + 33,147,904 B read,
+# 36,334,848 + 35,846,400 B written) and one 8192 x 8192 lattice, tile 16 x 8 (111,228,928 B read
 # + 253,859,584 B written).  Traffic grows with the sites swept, so other sizes scale by their
 # site count.
-ASSIGN_TRAFFIC_PER_SITE = {"kb_assign": (33_116_672 + 33_139_200 + 36_331_520 + 38_318_336) / 39_603_200,
+ASSIGN_TRAFFIC_PER_SITE = {"kb_assign": (33_125_632 + 33_147_904 + 36_334_848 + 35_846_400) / 39_603_200,
                            "k_assign": (111_228_928 + 253_859_584) / 8192 ** 2}
 
 
