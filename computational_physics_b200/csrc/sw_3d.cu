@@ -81,8 +81,11 @@ __host__ __device__ inline uint32_t draw_updates3(const Geo3 &g, uint32_t W)
 }
 
 struct Assign3Smem {
-    uint32_t parent, acc, box, face, total;
+    uint32_t parent, acc, box, face, pairs, total;
 };
+
+// Pending unions of the fixed-shape assign: a slice of this many words per warp.
+constexpr uint32_t k3PairCap = 192;
 
 __host__ __device__ inline Assign3Smem assign3_smem(const Geo3 &g)
 {
@@ -92,7 +95,8 @@ __host__ __device__ inline Assign3Smem assign3_smem(const Geo3 &g)
     s.acc = ns * 4;                                       // accepted draws: [3][ns] bytes, +x, +y, +z
     s.box = s.acc + 3 * ns;                               // spins of the block and its +1 halo
     s.face = (s.box + (g.BX + 1) * (g.BY + 1) * (g.BZ + 1) + 3) & ~3u;  // face bitmaps
-    s.total = s.face + 4 * face_words(g);
+    s.pairs = (s.face + 4 * face_words(g) + 15) & ~15u;
+    s.total = s.pairs + 4 * k3PairCap * (k3Threads / 32);
     return s;
 }
 
@@ -247,7 +251,57 @@ __global__ void __launch_bounds__(k3Threads) k3_assign(const Geo3 g_in, const ui
     }
     __syncthreads();
 
-    // ---- bonds (equal spins and an accepted draw); in-block unions, face bits for the merge
+    // ---- bonds (equal spins and an accepted draw); in-block unions, face bits for the merge.
+    // The fixed form queues a warp's unions in its slice of a shared list and runs them
+    // together, one per lane (inside the loop up to three unions ran, divergent, per site);
+    // the union-find's roots (each set's minimum) do not depend on the order of the unions.
+    if constexpr (kFixed) {
+        const uint32_t lane = tid & 31, below = (1u << lane) - 1u;
+        uint32_t *pl = reinterpret_cast<uint32_t *>(smem + S.pairs) + (tid >> 5) * k3PairCap;
+        uint32_t npend = 0;  // warp-uniform
+        auto flush = [&]() {
+            __syncwarp();
+            for (uint32_t i = lane; i < npend; i += 32) {
+                const uint32_t pr = pl[i];
+                uf_union(parent, pr & 0xFFFFu, pr >> 16);
+            }
+            __syncwarp();
+            npend = 0;
+        };
+        auto queue = [&](const bool u, const uint32_t a, const uint32_t b) {
+            const uint32_t m = __ballot_sync(0xffffffffu, u);
+            if (u)
+                pl[npend + __popc(m & below)] = a | b << 16;
+            npend += __popc(m);
+        };
+        for (uint32_t l = tid; l < NS; l += k3Threads) {  // every site of the block is on the lattice
+            const uint32_t zl = l / (BX * BY), yl = (l / BX) % BY, xl = l % BX;
+            const uint32_t b0 = zl * pxy + yl * px + xl;
+            const uint8_t s = box[b0];
+            const uint32_t bond = (acc[l] && s == box[b0 + 1]) | ((acc[NS + l] && s == box[b0 + px]) << 1) |
+                                  ((acc[2 * NS + l] && s == box[b0 + pxy]) << 2);
+            if (dump_bonds)
+                dump_bonds[((size_t)(z0 + zl) * g.L1 + y0 + yl) * g.L0 + x0 + xl] = (uint8_t)bond;
+            if ((bond & 1u) && xl + 1 == BX) {
+                const uint32_t f = zl * BY + yl;
+                atomicOr(face + (f >> 5), 1u << (f & 31));
+            }
+            if ((bond & 2u) && yl + 1 == BY) {
+                const uint32_t f = zl * BX + xl;
+                atomicOr(face + g.wx + (f >> 5), 1u << (f & 31));
+            }
+            if ((bond & 4u) && zl + 1 == BZ) {
+                const uint32_t f = yl * BX + xl;
+                atomicOr(face + g.wx + g.wy + (f >> 5), 1u << (f & 31));
+            }
+            queue((bond & 1u) && xl + 1 < BX, l, l + 1);
+            queue((bond & 2u) && yl + 1 < BY, l, l + BX);
+            queue((bond & 4u) && zl + 1 < BZ, l, l + BX * BY);
+            if (npend > k3PairCap - 96)  // room for the next site's three
+                flush();
+        }
+        flush();
+    } else
     for (uint32_t l = tid; l < NS; l += nthr) {
         const uint32_t zl = l / (BX * BY), yl = (l / BX) % BY, xl = l % BX;
         if (xl >= bxv || yl >= byv || zl >= bzv)
