@@ -413,12 +413,55 @@ __global__ void __launch_bounds__(k3Threads) k3_resolve(const Geo3 g, const uint
 
 // Every block root's label is its cluster's root after k3_resolve; every site reads its root's
 // and flips iff it is odd.  With write_labels the resolved labels are stored (a dumped sweep).
+// kFixed: every block a whole 32 x 8 x 8 block (the assign's fixed form): each thread holds two
+// quads of four sites (one 16-byte label load and one 4-byte spin load each) from the first pass
+// to the second.
+template <bool kFixed = false>
 __global__ void __launch_bounds__(k3Threads) k3_flip(const Geo3 g, uint8_t *__restrict__ spins, uint32_t *labels,
                                                       const int write_labels)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     uint32_t *res = reinterpret_cast<uint32_t *>(smem);
     const uint32_t bxi = blockIdx.x, byi = blockIdx.y, bzi = blockIdx.z;
+    if constexpr (kFixed) {
+        static_assert(k3Threads == 256, "two quads per thread over 2048 sites");
+        const uint32_t x0 = bxi * 32, y0 = byi * 8, z0 = bzi * 8;
+        uint4 lab[2];
+        uint32_t spn[2];
+        size_t site[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const uint32_t q = threadIdx.x + k * 256, r = q >> 3, x = (q & 7) * 4;  // row r = zl * 8 + yl
+            site[k] = ((size_t)(z0 + (r >> 3)) * g.L1 + y0 + (r & 7)) * g.L0 + x0 + x;
+            lab[k] = *reinterpret_cast<const uint4 *>(labels + site[k]);
+            spn[k] = *reinterpret_cast<const uint32_t *>(spins + site[k]);
+        }
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const uint32_t l = (threadIdx.x + k * 256) * 4;
+            const uint32_t v[4] = {lab[k].x, lab[k].y, lab[k].z, lab[k].w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (!(v[j] & kLocalFlag))
+                    res[l + j] = v[j];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const uint32_t l = (threadIdx.x + k * 256) * 4;
+            const uint32_t v[4] = {lab[k].x, lab[k].y, lab[k].z, lab[k].w};
+            uint32_t rr[4], flip = 0;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                rr[j] = res[(v[j] & kLocalFlag) ? (v[j] & kLocalMask) : l + j];
+                flip |= (rr[j] & 1u) << (8 * j);
+            }
+            *reinterpret_cast<uint32_t *>(spins + site[k]) = spn[k] ^ flip;
+            if (write_labels)
+                *reinterpret_cast<uint4 *>(labels + site[k]) = make_uint4(rr[0], rr[1], rr[2], rr[3]);
+        }
+        return;
+    }
     const uint32_t BX = g.BX, BY = g.BY, BZ = g.BZ, NS = BX * BY * BZ;
     const uint32_t x0 = bxi * BX, y0 = byi * BY, z0 = bzi * BZ;
     const uint32_t bxv = min(BX, g.L0 - x0), byv = min(BY, g.L1 - y0), bzv = min(BZ, g.L2 - z0);
@@ -559,7 +602,10 @@ int launch_sweep3(swb_lattice3 *h, float temperature, uint8_t *dump_bonds, bool 
     SWB_LAUNCHED();
     k3_resolve<<<grid, k3Threads, 0, h->stream>>>(g, h->linked, h->labels, h->fault);
     SWB_LAUNCHED();
-    k3_flip<<<grid, k3Threads, block_sites(g) * 4, h->stream>>>(g, h->spins, h->labels, write_labels ? 1 : 0);
+    if (fixed)
+        k3_flip<true><<<grid, k3Threads, block_sites(g) * 4, h->stream>>>(g, h->spins, h->labels, write_labels ? 1 : 0);
+    else
+        k3_flip<><<<grid, k3Threads, block_sites(g) * 4, h->stream>>>(g, h->spins, h->labels, write_labels ? 1 : 0);
     SWB_LAUNCHED();
     return SWB_OK;
 }
