@@ -41,7 +41,7 @@ struct Geo3 {
     uint32_t wx, wy, wz;        // words of the +x, +y, +z face bitmaps per block
 };
 
-// Blocks of about 2048 sites whose tiles' lcg lanes fit one CTA (tiles x W <= 256).
+// Blocks of about 4096 sites whose tiles' lcg lanes fit one CTA (tiles x W <= 256).
 inline Geo3 make_geo3(uint32_t L0, uint32_t L1, uint32_t L2, uint32_t TX, uint32_t TY, uint32_t TZ, uint32_t W)
 {
     Geo3 g{};
@@ -51,7 +51,7 @@ inline Geo3 make_geo3(uint32_t L0, uint32_t L1, uint32_t L2, uint32_t TX, uint32
     g.n2 = (L2 + TZ - 1) / TZ;
     g.TBX = std::max(1u, 32 / TX);
     g.TBY = std::max(1u, 8 / TY);
-    g.TBZ = std::max(1u, 8 / TZ);
+    g.TBZ = std::max(1u, 16 / TZ);
     while (g.TBX * g.TBY * g.TBZ * W > k3Threads) {
         if (g.TBZ > 1) g.TBZ /= 2;
         else if (g.TBY > 1) g.TBY /= 2;
@@ -110,7 +110,7 @@ __device__ __forceinline__ uint32_t label_global3(const Geo3 &g, uint32_t bxi, u
     return ((bzi * g.BZ + zl) * g.L1 + byi * g.BY + yl) * g.L0 + bxi * g.BX + xl;
 }
 
-// kFixed: tile 16 x 4 x 4, lcg width 16, and every block a full 32 x 8 x 8 block (the caller
+// kFixed: tile 16 x 4 x 4, lcg width 16, and every block a full 32 x 8 x 16 block (the caller
 // checked): the block and tile shape are constants, so the site index arithmetic is shifts and
 // the loops have fixed trip counts.
 template <int W, bool kFixed = false>
@@ -125,9 +125,9 @@ __global__ void __launch_bounds__(k3Threads) k3_assign(const Geo3 g_in, const ui
     Geo3 gfix = g_in;
     if constexpr (kFixed) {
         gfix.TX = 16; gfix.TY = 4; gfix.TZ = 4;
-        gfix.TBX = 2; gfix.TBY = 2; gfix.TBZ = 2;
-        gfix.BX = 32; gfix.BY = 8; gfix.BZ = 8;
-        gfix.wx = 2; gfix.wy = 8; gfix.wz = 8;
+        gfix.TBX = 2; gfix.TBY = 2; gfix.TBZ = 4;
+        gfix.BX = 32; gfix.BY = 8; gfix.BZ = 16;
+        gfix.wx = 4; gfix.wy = 16; gfix.wz = 8;
     }
     const Geo3 &g = kFixed ? gfix : g_in;
     const Assign3Smem S = assign3_smem(g);
@@ -413,7 +413,7 @@ __global__ void __launch_bounds__(k3Threads) k3_resolve(const Geo3 g, const uint
 
 // Every block root's label is its cluster's root after k3_resolve; every site reads its root's
 // and flips iff it is odd.  With write_labels the resolved labels are stored (a dumped sweep).
-// kFixed: every block a whole 32 x 8 x 8 block (the assign's fixed form): each thread holds two
+// kFixed: every block a whole 32 x 8 x 16 block (the assign's fixed form): each thread holds four
 // quads of four sites (one 16-byte label load and one 4-byte spin load each) from the first pass
 // to the second.
 template <bool kFixed = false>
@@ -424,20 +424,20 @@ __global__ void __launch_bounds__(k3Threads) k3_flip(const Geo3 g, uint8_t *__re
     uint32_t *res = reinterpret_cast<uint32_t *>(smem);
     const uint32_t bxi = blockIdx.x, byi = blockIdx.y, bzi = blockIdx.z;
     if constexpr (kFixed) {
-        static_assert(k3Threads == 256, "two quads per thread over 2048 sites");
-        const uint32_t x0 = bxi * 32, y0 = byi * 8, z0 = bzi * 8;
-        uint4 lab[2];
-        uint32_t spn[2];
-        size_t site[2];
+        static_assert(k3Threads == 256, "four quads per thread over 4096 sites");
+        const uint32_t x0 = bxi * 32, y0 = byi * 8, z0 = bzi * 16;
+        uint4 lab[4];
+        uint32_t spn[4];
+        size_t site[4];
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
+        for (int k = 0; k < 4; ++k) {
             const uint32_t q = threadIdx.x + k * 256, r = q >> 3, x = (q & 7) * 4;  // row r = zl * 8 + yl
             site[k] = ((size_t)(z0 + (r >> 3)) * g.L1 + y0 + (r & 7)) * g.L0 + x0 + x;
             lab[k] = *reinterpret_cast<const uint4 *>(labels + site[k]);
             spn[k] = *reinterpret_cast<const uint32_t *>(spins + site[k]);
         }
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
+        for (int k = 0; k < 4; ++k) {
             const uint32_t l = (threadIdx.x + k * 256) * 4;
             const uint32_t v[4] = {lab[k].x, lab[k].y, lab[k].z, lab[k].w};
 #pragma unroll
@@ -447,7 +447,7 @@ __global__ void __launch_bounds__(k3Threads) k3_flip(const Geo3 g, uint8_t *__re
         }
         __syncthreads();
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
+        for (int k = 0; k < 4; ++k) {
             const uint32_t l = (threadIdx.x + k * 256) * 4;
             const uint32_t v[4] = {lab[k].x, lab[k].y, lab[k].z, lab[k].w};
             uint32_t rr[4], flip = 0;
@@ -585,8 +585,8 @@ int launch_sweep3(swb_lattice3 *h, float temperature, uint8_t *dump_bonds, bool 
     const Geo3 &g = h->g;
     const dim3 grid(g.nbx, g.nby, g.nbz);
     const uint32_t thr = accept_threshold(swb_p_add(temperature));
-    const bool fixed = h->W == 16 && g.TX == 16 && g.TY == 4 && g.TZ == 4 && g.BX == 32 && g.BY == 8 && g.BZ == 8 &&
-                       g.L0 % 32 == 0 && g.L1 % 8 == 0 && g.L2 % 8 == 0;
+    const bool fixed = h->W == 16 && g.TX == 16 && g.TY == 4 && g.TZ == 4 && g.BX == 32 && g.BY == 8 && g.BZ == 16 &&
+                       g.L0 % 32 == 0 && g.L1 % 8 == 0 && g.L2 % 16 == 0;
     if (fixed)
         k3_assign<16, true><<<grid, k3Threads, h->smem_assign, h->stream>>>(g, h->spins, h->labels, h->rng_state,
                                                                             h->rng_sel, h->rng_iter, thr, h->faces,
